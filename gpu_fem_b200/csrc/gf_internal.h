@@ -1,0 +1,138 @@
+// Internal definitions shared by the libgpufem translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/gpufem.h"
+#include "shell_element.cuh"
+
+namespace gf {
+
+// Thread-local text of the last CUDA error seen by the library.
+void set_last_error(const char* where, cudaError_t e);
+
+#define GF_CUDA(call)                                  \
+  do {                                                 \
+    cudaError_t _e = (call);                           \
+    if (_e != cudaSuccess) {                           \
+      ::gf::set_last_error(#call, _e);                 \
+      return _e == cudaErrorMemoryAllocation ? GF_OOM : GF_CUDA_ERROR; \
+    }                                                  \
+  } while (0)
+
+#define GF_CHECK_LAUNCH()                              \
+  do {                                                 \
+    cudaError_t _e = cudaGetLastError();               \
+    if (_e != cudaSuccess) {                           \
+      ::gf::set_last_error("kernel launch", _e);       \
+      return GF_CUDA_ERROR;                            \
+    }                                                  \
+  } while (0)
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Device buffer that frees itself.
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  cudaError_t alloc(size_t count) {
+    release();
+    n = count;
+    if (count == 0) return cudaSuccess;
+    return cudaMalloc(&p, count * sizeof(T));
+  }
+  cudaError_t upload(const T* h, size_t count) {
+    cudaError_t e = alloc(count);
+    if (e != cudaSuccess || count == 0) return e;
+    return cudaMemcpy(p, h, count * sizeof(T), cudaMemcpyHostToDevice);
+  }
+  cudaError_t upload(const std::vector<T>& v) { return upload(v.data(), v.size()); }
+};
+
+// ---------------------------------------------------------------- symbolic
+struct Pattern {
+  int n = 0;
+  std::vector<int32_t> rowp, cols;
+  int nnz() const { return rowp.empty() ? 0 : rowp[n]; }
+};
+
+// Node adjacency through shared elements (get_row_col_ptrs,
+// include/linalg/bsr_utils.h:430-476).
+Pattern pattern_from_conn(int nelem, int nnodes, const int32_t* conn);
+// TacsComputeRCMOrder (include/linalg/reordering_utils.h:189-291): rcm[old] = new.
+void rcm_order(const Pattern& p, int root, int iters, std::vector<int32_t>& rcm);
+Pattern permute_pattern(const Pattern& p, const std::vector<int32_t>& perm);
+// get_elem_ind_map (include/linalg/bsr_utils.h:809-870); -1 if not found.
+void elem_ind_map(int nelem, const int32_t* conn, const Pattern& p,
+                  const std::vector<int32_t>& perm, std::vector<int32_t>& map);
+// computeILUk (include/linalg/bsr_utils.h:678-807).
+Pattern iluk_pattern(const Pattern& a, int lev);
+// Level sets of the lower / upper triangular DAG.
+int levels(const Pattern& p, bool lower, std::vector<int32_t>& level);
+
+// Coloured scatter schedule (this project's design; restated in the oracle).
+struct Schedule {
+  int chunk_size = 0;
+  int nchunks = 0, ncc = 0;      // chunks, chunk colours
+  int max_ec = 0;                // element colours (max over chunks)
+  std::vector<int32_t> elem_chunk, chunk_color, elem_color;
+  std::vector<uint32_t> first_touch;  // bits 0-15 blocks (4a+b), 16-19 nodes
+  // execution order
+  std::vector<int32_t> order;         // schedule position -> element
+  std::vector<int32_t> chunk_list;    // chunks sorted by (colour, id)
+  std::vector<int32_t> cc_start;      // [ncc+1] offsets into chunk_list
+  std::vector<int32_t> chunk_start;   // [nchunks+1] schedule offsets (in chunk_list order)
+  std::vector<int32_t> ec_off;        // [nchunks * (kMaxEC+1)] colour offsets within chunk
+};
+constexpr int kMaxEC = 15;
+int build_schedule(int nelem, int nnodes, const int32_t* conn, const std::vector<int32_t>& emap,
+                   int nnzb, int chunk_size, Schedule& s);
+
+}  // namespace gf
+
+// ------------------------------------------------------------------ handles
+struct gf_assembler {
+  int nnodes = 0, nelem = 0, nbcs = 0;
+  gf::Pattern pat0;                 // natural pattern
+  gf::Pattern pat;                  // solver-order pattern
+  std::vector<int32_t> perm, iperm;
+  std::vector<int32_t> conn;        // natural
+  std::vector<int32_t> bcs;
+  std::vector<int32_t> emap;        // natural element order
+  gf::Schedule sched;
+  std::vector<gf::Material> mats;
+  // device: natural-order mesh
+  gf::DevBuf<double> d_xpts, d_vars;
+  gf::DevBuf<int32_t> d_perm, d_bcs;
+  gf::DevBuf<uint8_t> d_bcmask;     // per natural node, bit r = DOF r constrained
+  // device: schedule-ordered element data
+  gf::DevBuf<int32_t> d_sconn, d_semap, d_smat;
+  gf::DevBuf<uint32_t> d_sft;
+  gf::DevBuf<double> d_sthick;
+  gf::DevBuf<int32_t> d_chunk_list, d_chunk_start, d_ec_off;
+  gf::DevBuf<gf::Material> d_mats;
+  // device: pattern (solver order) and BC entry list
+  gf::DevBuf<int32_t> d_rowp, d_cols;
+  gf::DevBuf<int32_t> d_bc_entries;  // 4 ints per entry: blk, row node, is_col, inner
+  int nbc_entries = 0;
+  gf::DevBuf<double> d_energy_part;
+  gf::DevBuf<int32_t> d_diag;        // solver-order diagonal block index per row
+};
+
+struct gf_bsr {
+  gf_assembler* a = nullptr;
+  gf::DevBuf<double> vals;
+};

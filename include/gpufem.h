@@ -1,0 +1,203 @@
+/*
+ * gpufem.h — C ABI of the B200 shell-analysis hot path (libgpufem.so).
+ *
+ * The reference (smdogroup/gpu_fem) is a header-only C++ template library
+ * with no C ABI; each entry point below replaces the member function or
+ * driver step cited beside it. A C++ facade that keeps the reference's class
+ * names (ElementAssembler, BsrMat, DeviceVec, HostVec, ILUk_Preconditioner)
+ * lives in include/gpufem/gpufem.hpp.
+ *
+ * Conventions
+ *  - All functions return gf_status; nothing calls exit().
+ *  - Device pointers are caller-owned and never freed by the library.
+ *    Handles (gf_assembler, gf_bsr, gf_precond, gf_solver, gf_batch) are
+ *    library-owned and released with their destroy call.
+ *  - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *    Work on distinct handles may run concurrently from different threads.
+ *  - Nodal vectors at the boundary are in the caller's (natural) node order,
+ *    6 DOF per node, AoS (6*node + dof) as in include/linalg/vec.h:47-57.
+ *    The BSR matrix is stored in the solver ordering (perm[old] = new), with
+ *    6x6 row-major blocks values[36*blk + 6*r + c] (include/linalg/bsr_mat.h:217-223)
+ *    and 32-bit rowPtr/colPtr (include/linalg/bsr_utils.h:16).
+ *  - All assembly arithmetic is FP64.
+ */
+#ifndef GPUFEM_H
+#define GPUFEM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum gf_status {
+  GF_OK = 0,
+  GF_INVALID_ARG = 1,
+  GF_OOM = 2,
+  GF_ZERO_PIVOT = 3,
+  GF_NOT_CONVERGED = 4,
+  GF_NAN = 5,
+  GF_TIMEOUT = 6,
+  GF_CUDA_ERROR = 7,
+  GF_NO_DEVICE = 8,
+  GF_OVER_BUDGET = 9
+} gf_status;
+
+/* Per-element isotropic shell data; same fields and meaning as
+ * ShellIsotropicData (include/shell/data.h:8-47). */
+typedef struct gf_shell_data {
+  double E, nu, thick, tOffset;
+  double refAxis[3];
+  int32_t has_ref_axis;
+  int32_t pad;
+} gf_shell_data;
+
+/* Mesh description (host arrays, copied by gf_assembler_create). Replaces
+ * the ElementAssembler constructor arguments (include/assembler.h:31-34). */
+typedef struct gf_mesh_desc {
+  int32_t num_nodes;           /* num_geo_nodes == num_vars_nodes */
+  int32_t num_elements;
+  const int32_t* conn;         /* 4 per element, tensor-product node order */
+  const double* xpts;          /* 3 per node */
+  const int32_t* bcs;          /* natural DOF indices (6*node + dof) */
+  int32_t num_bcs;
+  const gf_shell_data* data;   /* one per element */
+  int32_t ordering;            /* GF_ORDER_* */
+  int32_t rcm_root;            /* RCM root node (reference uses 0) */
+} gf_mesh_desc;
+
+enum { GF_ORDER_NATURAL = 0, GF_ORDER_RCM = 1 };
+
+enum { GF_ASSEMBLE_OVERWRITE = 0, GF_ASSEMBLE_ADD = 1, GF_ASSEMBLE_FUSE_BCS = 2 };
+
+typedef struct gf_assembler gf_assembler;
+typedef struct gf_bsr gf_bsr;
+typedef struct gf_precond gf_precond;
+
+/* ---- library --------------------------------------------------------- */
+const char* gf_status_string(gf_status s);
+const char* gf_version(void);
+/* Last CUDA error text seen by the library on this thread ("" if none). */
+const char* gf_last_error(void);
+
+/* ---- assembler ------------------------------------------------------- */
+/* ElementAssembler(...) (include/assembler.h:31-73) + BsrData(...)
+ * (include/linalg/bsr_utils.h:46-62) + post_reordering_update (:84-103).
+ * Builds the block pattern, the optional RCM ordering
+ * (include/linalg/reordering_utils.h:272-291), elemIndMap
+ * (include/linalg/bsr_utils.h:809-870), the coloured scatter schedule and
+ * uploads the mesh to the current device. */
+gf_status gf_assembler_create(const gf_mesh_desc* desc, gf_assembler** out);
+gf_status gf_assembler_destroy(gf_assembler* a);
+/* get_num_nodes / get_num_elements / get_num_vars (include/assembler.h:117-118, :309-310) */
+int32_t gf_assembler_num_nodes(const gf_assembler* a);
+int32_t gf_assembler_num_elements(const gf_assembler* a);
+int32_t gf_assembler_num_vars(const gf_assembler* a);
+int32_t gf_assembler_nnzb(const gf_assembler* a);
+/* BsrData public fields (include/linalg/bsr_utils.h:395-403), host copies:
+ * rowPtr[nnodes+1], colPtr[nnzb], perm[nnodes] (perm[old] = new),
+ * elemIndMap[16*nelems]; any pointer may be NULL. */
+gf_status gf_assembler_get_pattern(const gf_assembler* a, int32_t* rowPtr, int32_t* colPtr,
+                                   int32_t* perm, int32_t* elemIndMap);
+/* Scatter schedule: chunk id, chunk colour, element colour and first-touch
+ * mask per element; chunk colour / element colour counts. Host copies. */
+gf_status gf_assembler_get_schedule(const gf_assembler* a, int32_t* elem_chunk,
+                                    int32_t* chunk_color, int32_t* elem_color,
+                                    uint32_t* first_touch, int32_t* num_chunk_colors,
+                                    int32_t* num_chunks);
+/* set_variables (include/assembler.h:191-195): d_vars is natural-order,
+ * 6*num_nodes doubles on the device; copied (not referenced). */
+gf_status gf_set_variables(gf_assembler* a, const double* d_vars, void* stream);
+/* add_residual (include/assembler.h:232-264, kernel base/elem_group.cuh:17-97):
+ * d_res (natural order) = R(u)  (or += with GF_ASSEMBLE_ADD). */
+gf_status gf_add_residual(gf_assembler* a, double* d_res, int32_t flags, void* stream);
+/* add_jacobian (include/assembler.h:267-305, kernel base/elem_group.cuh:103-211):
+ * K(u) into the BSR values (overwrite, or += with GF_ASSEMBLE_ADD) and R(u)
+ * into d_res (may be NULL). GF_ASSEMBLE_FUSE_BCS applies the Dirichlet
+ * rows/columns of apply_bcs(Mat) and zeroes BC entries of d_res in the same
+ * pass. */
+gf_status gf_add_jacobian(gf_assembler* a, double* d_res, gf_bsr* mat, int32_t flags,
+                          void* stream);
+/* add_energy (include/assembler.h:198-229; the reference GPU kernel is an
+ * empty stub, base/elem_group.cuh:11-13): *h_energy = U(u). */
+gf_status gf_add_energy(gf_assembler* a, double* h_energy, void* stream);
+/* apply_bcs(Vec) (include/assembler.h:119-136, vec.cuh:3-13). */
+gf_status gf_apply_bcs_vec(gf_assembler* a, double* d_vec, void* stream);
+/* apply_bcs(Mat) (include/assembler.h:137-154, bsr_mat.cuh:1-104). */
+gf_status gf_apply_bcs_mat(gf_assembler* a, gf_bsr* mat, void* stream);
+
+/* ---- BSR matrix ------------------------------------------------------ */
+/* createBsrMat (include/linalg/bsr_mat.h:354-357): values zeroed. */
+gf_status gf_bsr_create(gf_assembler* a, gf_bsr** out);
+gf_status gf_bsr_destroy(gf_bsr* m);
+/* getPtr (bsr_mat.h:31-32): device pointer to nnzb*36 doubles. */
+double* gf_bsr_values(gf_bsr* m);
+gf_status gf_bsr_zero(gf_bsr* m, void* stream);
+/* cusparseDbsrmv as used at examples/iterative/gmres.cu:498-509:
+ * y = alpha A x + beta y, vectors in the solver ordering. */
+gf_status gf_bsr_spmv(gf_bsr* m, double alpha, const double* d_x, double beta, double* d_y,
+                      void* stream);
+/* Natural-order <-> solver-order vector permutation (permute_vec_kernel,
+ * vec.cuh:15-34; bsr_pre_solve / bsr_post_solve, solve_utils.h:4-17).
+ * direction 0: out[perm[i]] = in[i]; 1: out[i] = in[perm[i]]. */
+gf_status gf_permute_vec(gf_assembler* a, const double* d_in, double* d_out, int32_t direction,
+                         void* stream);
+
+/* ---- ILU preconditioner ---------------------------------------------- */
+enum { GF_PREC_FP64 = 0, GF_PREC_FP32 = 1 };
+/* ILUk_Preconditioner (include/linalg/precond.h:5-55) with the symbolic
+ * ILU(k) of computeILUk (include/linalg/bsr_utils.h:678-807); fill_level 0
+ * keeps A's pattern (ILU(0)). precision selects FP64 or FP32 factors. */
+gf_status gf_precond_create(gf_assembler* a, int32_t fill_level, int32_t precision,
+                            gf_precond** out);
+gf_status gf_precond_destroy(gf_precond* p);
+/* copyValues + numeric factorization (precond.h:35-44; cusparseDbsrilu02 at
+ * examples/iterative/gmres.cu:426-457). Level-scheduled on the device. */
+gf_status gf_precond_factor(gf_precond* p, gf_bsr* A, void* stream);
+/* z = U^{-1} L^{-1} r (two cusparseDbsrsv2_solve calls,
+ * examples/iterative/gmres.cu:522-532), solver ordering. */
+gf_status gf_precond_apply(gf_precond* p, const double* d_r, double* d_z, void* stream);
+/* Pattern, level count and factor copy for checking. rowPtr/colPtr may be
+ * NULL; values receives nnzb_pc*36 entries with the diagonal blocks holding
+ * U_ii^{-1}. */
+gf_status gf_precond_info(const gf_precond* p, int32_t* nnzb, int32_t* num_levels_L,
+                          int32_t* num_levels_U);
+gf_status gf_precond_get(const gf_precond* p, int32_t* rowPtr, int32_t* colPtr,
+                         double* h_values);
+
+/* ---- GMRES / iterative refinement ------------------------------------ */
+typedef struct gf_solve_opts {
+  int32_t restart;        /* m (reference: 30, examples/iterative/gmres.cu:33) */
+  int32_t max_iters;      /* total Arnoldi steps */
+  double rtol;            /* ||b - A x||_2 / ||b||_2 target (FP64 A) */
+  int32_t side;           /* 0 left (reference), 1 right preconditioning */
+  int32_t mixed;          /* 0: FP64 GMRES; 1: FP32 SpMV + FP32 ILU inside
+                              FP64 GMRES with FP64 iterative refinement */
+  double inner_rtol;      /* inner tolerance per refinement step (mixed) */
+  int32_t max_refine;     /* max refinement steps (mixed) */
+  int32_t check_every;    /* host polls convergence every k steps */
+} gf_solve_opts;
+
+typedef struct gf_solve_stats {
+  int32_t iterations;     /* Arnoldi steps */
+  int32_t restarts;
+  int32_t refinements;
+  int32_t status;         /* gf_status of the solve */
+  double rel_residual;    /* final ||b - A x|| / ||b|| in FP64 */
+  double time_ms;
+} gf_solve_stats;
+
+void gf_solve_opts_default(gf_solve_opts* o);
+/* The ILU-GMRES driver of examples/iterative/gmres.cu:468-771 (bugs fixed:
+ * dot length nvars, m+1 basis vectors, restarts): solves A x = b with the
+ * BSR matrix A (BCs applied) and a factored preconditioner. d_b / d_x are in
+ * natural order; permutation happens inside. d_x is the initial guess on
+ * entry. Device-resident: no host round trip per Arnoldi step. */
+gf_status gf_gmres_solve(gf_assembler* a, gf_bsr* A, gf_precond* p, const double* d_b,
+                         double* d_x, const gf_solve_opts* opts, gf_solve_stats* stats,
+                         void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPUFEM_H */

@@ -1,0 +1,120 @@
+"""GPU parity of SpMV, block ILU(k), triangular solves and GMRES."""
+import numpy as np
+import pytest
+
+from gpu_fem_b200 import mesh as M
+
+pytestmark = pytest.mark.gpu
+
+
+def _system(mesh, ordering, oracle):
+    import torch
+    from gpu_fem_b200.assembler import ElementAssembler, createBsrMat
+    A = ElementAssembler.from_mesh(mesh, ordering=ordering)
+    K = createBsrMat(A)
+    A.add_jacobian(None, K, fuse_bcs=True)
+    torch.cuda.synchronize()
+    bd = A.getBsrData()
+    rowp, cols, vals, _, perm = oracle.assemble_jacobian(mesh, perm=bd["perm"])
+    oracle.apply_bcs_mat(rowp, cols, vals, perm, mesh.bcs)
+    return A, K, rowp, cols, vals, perm
+
+
+def _to_solver(v, perm):
+    out = np.zeros_like(v)
+    out.reshape(-1, 6)[perm] = v.reshape(-1, 6)
+    return out
+
+
+def test_spmv_matches_oracle(oracle):
+    import torch
+    mesh = M.plate_config2(24, 12)
+    A, K, rowp, cols, vals, perm = _system(mesh, "rcm", oracle)
+    x = np.random.default_rng(1).standard_normal(mesh.num_dof)
+    y_ref = oracle.spmv(rowp, cols, vals, x)
+    xt = torch.tensor(x, device="cuda")
+    yt = torch.zeros_like(xt)
+    K.spmv(xt, yt)
+    y = yt.cpu().numpy()
+    assert np.abs(y - y_ref).max() <= 1e-13 * np.abs(y_ref).max()
+
+
+@pytest.mark.parametrize("fill", [0, 2])
+def test_ilu_factor_and_apply_match_oracle(oracle, fill):
+    import torch
+    from gpu_fem_b200.assembler import ILUk_Preconditioner
+    mesh = M.plate_config2(24, 12)
+    A, K, rowp, cols, vals, perm = _system(mesh, "rcm", oracle)
+    P = ILUk_Preconditioner(A, fill_level=fill)
+    P.factor(K)
+    torch.cuda.synchronize()
+    r2, c2, lu_gpu = P.get()
+    if fill:
+        rk, ck = oracle.iluk_pattern(rowp, cols, fill)
+        np.testing.assert_array_equal(r2, rk)
+        np.testing.assert_array_equal(c2, ck)
+        vals_k = oracle.scatter_to_pattern(rowp, cols, vals, rk, ck)
+    else:
+        np.testing.assert_array_equal(r2, rowp)
+        np.testing.assert_array_equal(c2, cols)
+        vals_k = vals
+    st, lu_ref = oracle.ilu0(r2, c2, vals_k)
+    assert st == 0
+    # off-diagonal blocks compare directly; the GPU stores U_ii^{-1}
+    n = len(r2) - 1
+    G = lu_gpu.reshape(-1, 6, 6)
+    R = lu_ref.reshape(-1, 6, 6)
+    scale = np.abs(R).max()
+    for i in range(n):
+        for jp in range(r2[i], r2[i + 1]):
+            if c2[jp] == i:
+                np.testing.assert_allclose(G[jp] @ R[jp], np.eye(6), atol=1e-9)
+            else:
+                assert np.abs(G[jp] - R[jp]).max() <= 1e-10 * scale
+    r = np.random.default_rng(2).standard_normal(mesh.num_dof)
+    z_ref = oracle.ilu0_apply(r2, c2, lu_ref, r)
+    rt = torch.tensor(r, device="cuda")
+    zt = torch.zeros_like(rt)
+    P.apply(rt, zt)
+    z = zt.cpu().numpy()
+    assert np.abs(z - z_ref).max() <= 1e-9 * np.abs(z_ref).max()
+
+
+@pytest.mark.parametrize("side", [0, 1])
+def test_gmres_config1_matches_dense_solve(oracle, side):
+    import torch
+    from gpu_fem_b200.assembler import ILUk_Preconditioner, SolveOptions, gmres_solve
+    mesh = M.plate_config1()
+    A, K, rowp, cols, vals, perm = _system(mesh, "natural", oracle)
+    x_dense = oracle.dense_solve(oracle.bsr_to_dense(rowp, cols, vals), mesh.loads)
+    P = ILUk_Preconditioner(A, fill_level=0)
+    P.factor(K)
+    b = torch.tensor(mesh.loads, device="cuda")
+    x = torch.zeros_like(b)
+    st, stats = gmres_solve(A, K, P, b, x, SolveOptions(restart=300, max_iters=3000, rtol=1e-10,
+                                                        side=side))
+    assert stats["rel_residual"] <= 1e-9, stats
+    err = np.linalg.norm(x.cpu().numpy() - x_dense) / np.linalg.norm(x_dense)
+    assert err <= 1e-8, (err, stats)
+
+
+def test_mixed_precision_refinement_reaches_fp64_tolerance(oracle):
+    import torch
+    from gpu_fem_b200.assembler import ILUk_Preconditioner, SolveOptions, gmres_solve
+    mesh = M.plate(32, 32, 1.0, 1.0, lambda x, y: 0.005 + 0 * x, "all_edges",
+                   lambda q: 1e3 + 0 * q[:, 0])
+    A, K, rowp, cols, vals, perm = _system(mesh, "rcm", oracle)
+    x_dense = oracle.dense_solve(oracle.bsr_to_dense(rowp, cols, vals),
+                                 _to_solver(mesh.loads, perm))
+    x_dense = x_dense.reshape(-1, 6)[perm].ravel()
+    b = torch.tensor(mesh.loads, device="cuda")
+    for mixed, prec in ((0, "fp64"), (1, "fp32")):
+        P = ILUk_Preconditioner(A, fill_level=2, precision=prec)
+        P.factor(K)
+        x = torch.zeros_like(b)
+        st, stats = gmres_solve(A, K, P, b, x, SolveOptions(restart=200, max_iters=4000,
+                                                            rtol=1e-8, mixed=mixed, side=1,
+                                                            inner_rtol=1e-3))
+        assert stats["rel_residual"] <= 1e-8, (mixed, stats)
+        err = np.linalg.norm(x.cpu().numpy() - x_dense) / np.linalg.norm(x_dense)
+        assert err <= 1e-6, (mixed, err, stats)

@@ -1,0 +1,46 @@
+"""Synthetic workload generators: sizes, tensor node order, seeds."""
+import numpy as np
+
+from gpu_fem_b200 import mesh as M
+
+
+def _normals_positive(mesh):
+    X = mesh.xpts[mesh.conn]
+    n = np.cross(X[:, 1] - X[:, 0], X[:, 2] - X[:, 0])
+    return (np.linalg.norm(n, axis=1) > 0).all()
+
+
+def test_config1_sizes():
+    m = M.plate_config1()
+    assert (m.num_nodes, m.num_elements, m.num_dof) == (121, 100, 726)
+    assert len(m.bcs) == 6 * 40
+    # 81 interior nodes carry h^2 p = 0.01 m^2 * 1 kPa each
+    assert abs(m.loads.sum() - 810.0) < 1e-9
+
+
+def test_config2_sizes_and_jitter():
+    m = M.plate_config2()
+    assert (m.num_nodes, m.num_elements) == (80601, 80000)
+    h = 0.005
+    ix = np.rint(m.xpts[:, 0] / h)
+    assert np.abs(m.xpts[:, 0] - ix * h).max() <= 0.1 * h + 1e-15
+    assert m.thick.min() >= 0.004 * 0.75 - 1e-12 and m.thick.max() <= 0.004 * 1.25 + 1e-12
+    assert _normals_positive(m)
+    # corners fixed, deterministic
+    m2 = M.plate_config2()
+    assert np.array_equal(m.xpts, m2.xpts)
+
+
+def test_box_small_topology():
+    b = M.box(nx=18, ny=6, nz=4, nribs=4)
+    assert b.num_elements == 2 * 18 * 6 + 2 * 18 * 4 + 4 * 6 * 4
+    assert _normals_positive(b)
+    assert abs(b.loads.sum() - 1e4) < 1e-6
+
+
+def test_batch_config4_seeded():
+    probs = M.batch_config4()
+    assert len(probs) == 64
+    sizes = [p.num_elements for p in probs]
+    assert min(sizes) >= 16 * 16 and max(sizes) <= 256 * 256
+    assert sizes == [p.num_elements for p in M.batch_config4()]
