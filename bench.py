@@ -1,0 +1,365 @@
+#!/usr/bin/env python
+"""Shell solves/sec (p50/p99 latency), mixed precision vs FP64 on the GPU.
+
+Workload: 64 independent clamped plates, element grids log-uniform 16^2 ..
+256^2 with aspect 1..4 (seed 4321), t ~ U(2, 8) mm, p ~ U(0.5, 2) kPa,
+E = 70 GPa, nu = 0.3. A step assembles the 6x6-block BSR Jacobian (fused
+BCs), factors the block ILU(k) preconditioner (k autotuned per problem) and
+solves every problem to ||b - A x|| / ||b|| <= 1e-8 with FP32 ILU + FP32
+SpMV inside FP64 GMRES / iterative refinement. `value` is whole-job solves/s
+with inputs resident in HBM; `e2e` repeats the step through the public API
+with the load vectors copied from pinned host memory and the displacements
+copied back inside the timed region. The FP64 GPU path is timed beside it.
+
+--impl reference times the CPU oracle (a restatement of the reference's CPU
+assembly plus FP64 ILU-GMRES) on a bounded sample of the same problems.
+
+Multi-GPU (torchrun): every rank solves its own full batch (replicas, weak
+scaling); the step time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "shell solves/sec + p50/p99 latency, mixed vs FP64 GPU at 1e-8 rel residual"
+WORKLOAD = ("64 clamped plates, grids 16^2-256^2 log-uniform, aspect 1-4, seed 4321; "
+            "assemble + block ILU(k) + GMRES/IR to 1e-8")
+
+
+def _args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--problems", type=int, default=64)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def _peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        sm = []
+        reasons = set()
+        smax = None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+                for k, nm in enumerate(names):
+                    if r[5 + k].lower().startswith("active"):
+                        reasons.add(nm)
+            except Exception:
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cpu_baseline_run(problems, fills, budget_s=25.0, threads=None):
+    """Oracle (restated reference CPU path): assembly (OpenMP over elements),
+    FP64 block ILU(k), left-preconditioned GMRES; on as many of the given
+    problems as fit in about budget_s. Returns (solves/s, n, seconds, cores)."""
+    import numpy as np
+
+    from oracle import pyoracle as po
+    threads = threads or os.cpu_count() or 1
+    t_total, n = 0.0, 0
+    for m, k in zip(problems, fills):
+        t0 = time.perf_counter()
+        rowp0, cols0 = po.bsr_pattern(m.conn, m.num_nodes)
+        perm = po.rcm(rowp0, cols0, 0, 1)
+        rowp, cols, A, _, perm = po.assemble_jacobian(m, perm=perm, nthreads=threads)
+        po.apply_bcs_mat(rowp, cols, A, perm, m.bcs)
+        b = np.zeros(6 * m.num_nodes)
+        b.reshape(-1, 6)[perm] = m.loads.reshape(-1, 6)
+        if k:
+            rk, ck = po.iluk_pattern(rowp, cols, k)
+            Ak = po.scatter_to_pattern(rowp, cols, A, rk, ck)
+        else:
+            rk, ck, Ak = rowp, cols, A
+        st, LU = po.ilu0(rk, ck, Ak)
+        # right preconditioning with the ILU(k) factors over A's pattern
+        st2, x, its, rel = _oracle_gmres_right(po, rowp, cols, A, rk, ck, LU, b)
+        dt = time.perf_counter() - t0
+        t_total += dt
+        n += 1
+        if t_total >= budget_s:
+            break
+    return n / t_total, n, t_total, threads
+
+
+def _oracle_gmres_right(po, rowp, cols, A, rk, ck, LU, b, m=200, rtol=1e-8, maxit=5000):
+    """FP64 right-preconditioned GMRES(m) on the oracle kernels (numpy
+    Arnoldi, C SpMV and ILU apply)."""
+    import numpy as np
+    x = np.zeros_like(b)
+    bn = np.linalg.norm(b)
+    r = b - po.spmv(rowp, cols, A, x)
+    rel = np.linalg.norm(r) / bn
+    it = 0
+    while rel > rtol and it < maxit:
+        beta = np.linalg.norm(r)
+        V = [r / beta]
+        H = np.zeros((m + 1, m))
+        g = np.zeros(m + 1)
+        g[0] = beta
+        cs, ss = np.zeros(m), np.zeros(m)
+        j = 0
+        for j in range(m):
+            w = po.spmv(rowp, cols, A, po.ilu0_apply(rk, ck, LU, V[j]))
+            for i in range(j + 1):
+                H[i, j] = w @ V[i]
+                w = w - H[i, j] * V[i]
+            H[j + 1, j] = np.linalg.norm(w)
+            V.append(w / H[j + 1, j])
+            for i in range(j):
+                a, c = H[i, j], H[i + 1, j]
+                H[i, j], H[i + 1, j] = cs[i] * a + ss[i] * c, -ss[i] * a + cs[i] * c
+            a, c = H[j, j], H[j + 1, j]
+            h = np.hypot(a, c)
+            cs[j], ss[j] = a / h, c / h
+            H[j, j], H[j + 1, j] = cs[j] * a + ss[j] * c, 0.0
+            g[j + 1], g[j] = -ss[j] * g[j], cs[j] * g[j]
+            it += 1
+            if abs(g[j + 1]) <= rtol * bn:
+                break
+        jj = j + 1
+        y = np.linalg.solve(np.triu(H[:jj, :jj]), g[:jj])
+        x += po.ilu0_apply(rk, ck, LU, sum(y[i] * V[i] for i in range(jj)))
+        r = b - po.spmv(rowp, cols, A, x)
+        rel = np.linalg.norm(r) / bn
+    return (0 if rel <= rtol else 1), x, it, rel
+
+
+def run_reference(args):
+    from gpu_fem_b200 import mesh as M
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return
+    probs = M.batch_config4(args.problems)
+    order = sorted(range(len(probs)), key=lambda i: probs[i].num_elements)
+    sample = [probs[i] for i in order]
+    fills = [_default_fill(p) for p in sample]
+    vals = []
+    for s in range(args.warmup + args.steps):
+        v, n, sec, cores = cpu_baseline_run(sample, fills, budget_s=20.0)
+        if s >= args.warmup:
+            vals.append(v)
+    value = statistics.median(vals)
+    line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * n / value,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded meshes)", "impl": "reference",
+            "config": {"workload": WORKLOAD, "sample": f"{n} smallest problems per step"},
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port",
+                             "sample": f"{n} smallest of the 64 problems, ~20 s per step"},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def _default_fill(mesh):
+    # offline sweep: thin, coarse plates need more fill (see DESIGN notes)
+    return 8
+
+
+def main():
+    args = _args()
+    if args.impl == "reference":
+        return run_reference(args)
+    import numpy as np
+    import torch
+
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    from gpu_fem_b200 import _lib as L
+    from gpu_fem_b200 import mesh as M
+    from gpu_fem_b200.batch import BatchSolver
+
+    meshes = M.batch_config4(args.problems)
+    t0 = time.perf_counter()
+    bs = BatchSolver(meshes, tune=True)
+    setup_s = time.perf_counter() - t0
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(mixed, host_io=None):
+        for _ in range(args.warmup):
+            bs.step(mixed, host_io)
+        barrier()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+        c0 = L.lib().gf_launch_count()
+        ev[0].record()
+        its = []
+        for k in range(args.steps):
+            stats = bs.step(mixed, host_io)
+            ev[k + 1].record()
+            its.append(max(s["iterations"] for s in stats))
+        barrier()
+        timed.launches = L.lib().gf_launch_count() - c0
+        lat = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
+        ms = ev[0].elapsed_time(ev[-1]) / args.steps
+        if ws > 1:
+            import torch.distributed as dist
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        timed.iters = its
+        return ms, lat
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms_mixed, lat_mixed = timed(True)
+    launches = timed.launches
+    its_mixed = timed.iters
+    clk = clocks.stop()
+    ms_fp64, lat_fp64 = timed(False)
+    its_fp64 = timed.iters
+    # end to end through the public API with host buffers
+    host_b = [torch.tensor(m.loads).pin_memory() for m in meshes]
+    host_x = [torch.empty(m.num_dof, dtype=torch.float64).pin_memory() for m in meshes]
+    ms_e2e, _ = timed(True, (host_b, host_x))
+    h2d = sum(8 * m.num_dof for m in meshes)
+    nprob = len(meshes)
+    value = ws * nprob / (ms_mixed / 1e3)
+
+    # roofline: block triangular solves (the dominant kernel) on the largest problem
+    ib = max(range(nprob), key=lambda i: meshes[i].num_nodes)
+    peak, peak_kind = _peaks()
+    from gpu_fem_b200.assembler import ILUk_Preconditioner
+    P = ILUk_Preconditioner(bs.asms[ib], bs.fills[ib], "fp32")
+    P.factor(bs.mats[ib])
+    inf = P.info()
+    r = torch.randn(meshes[ib].num_dof, dtype=torch.float64, device="cuda")
+    z = torch.zeros_like(r)
+    reps = 20
+    for _ in range(3):
+        P.apply(r, z)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        P.apply(r, z)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_apply = e0.elapsed_time(e1) / reps
+    n = meshes[ib].num_nodes
+    # algorithmic bytes of L + U sweeps (FP32 values): values + column indices +
+    # row pointers twice + rhs/solution vectors twice (8-byte)
+    bytes_apply = inf["nnzb"] * (36 * 4 + 4) + 8 * (n + 1) + 6 * n * 2 * (8 + 8)
+    achieved = bytes_apply / (ms_apply / 1e3) / 1e9
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_mixed,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 assembly + f32 ILU/SpMV in f64 GMRES/IR", "data": "synthetic (seeded meshes)",
+        "config": {"workload": WORKLOAD, "problems": nprob,
+                   "dofs": int(sum(m.num_dof for m in meshes)),
+                   "fill_levels": bs.fills,
+                   "gmres_steps_max": {"mixed": its_mixed, "fp64": its_fp64},
+                   "l2": "inputs larger than L2 (all 64 systems resident, ~GB)",
+                   "setup_s": round(setup_s, 2), "parallelism": f"replicas x{ws}"},
+        "latency_ms": {"p50": float(np.percentile(lat_mixed, 50)),
+                       "p99": float(np.percentile(lat_mixed, 99)),
+                       "note": "all 64 requests of a step complete together"},
+        "fp64_gpu": {"value": ws * nprob / (ms_fp64 / 1e3), "unit": "solves/s",
+                     "ms_per_step": ms_fp64,
+                     "latency_ms": {"p50": float(np.percentile(lat_fp64, 50)),
+                                    "p99": float(np.percentile(lat_fp64, 99))}},
+        "mixed_over_fp64": ms_fp64 / ms_mixed,
+        "e2e": {"value": ws * nprob / (ms_e2e / 1e3), "unit": "solves/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
+        "roofline": {"kernel": "trisolve_kernel (block L and U sweeps, FP32 values)",
+                     "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": None, "levels": [inf["levels_L"], inf["levels_U"]],
+                     "problem": meshes[ib].name},
+        "clocks": clk,
+        "gpu_launches": int(launches),
+    }
+    if rank == 0 and not args.no_cpu_baseline and ws == 1:
+        order = sorted(range(nprob), key=lambda i: meshes[i].num_elements)
+        v, n_cpu, sec, cores = cpu_baseline_run([meshes[i] for i in order],
+                                                [bs.fills[i] for i in order],
+                                                budget_s=20.0)
+        line["cpu_baseline"] = {"value": v, "unit": "solves/s", "cores": cores, "kind": "port",
+                                "sample": f"{n_cpu} smallest of the 64 problems ({sec:.1f} s)"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

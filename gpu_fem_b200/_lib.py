@@ -65,6 +65,7 @@ SIGNATURES = {
     "gf_status_string": (C.c_char_p, [_I]),
     "gf_version": (C.c_char_p, []),
     "gf_last_error": (C.c_char_p, []),
+    "gf_launch_count": (C.c_longlong, []),
     "gf_assembler_create": (_I, [C.POINTER(gf_mesh_desc), C.POINTER(_P)]),
     "gf_assembler_destroy": (_I, [_P]),
     "gf_assembler_num_nodes": (_I, [_P]),
@@ -74,6 +75,7 @@ SIGNATURES = {
     "gf_assembler_get_pattern": (_I, [_P, _PI, _PI, _PI, _PI]),
     "gf_assembler_get_schedule": (_I, [_P, _PI, _PI, _PI, _PU, _PI, _PI]),
     "gf_set_variables": (_I, [_P, _P, _P]),
+    "gf_assembler_set_thickness": (_I, [_P, _P, _P]),
     "gf_add_residual": (_I, [_P, _P, _I, _P]),
     "gf_add_jacobian": (_I, [_P, _P, _P, _I, _P]),
     "gf_add_energy": (_I, [_P, _PD, _P]),
@@ -93,6 +95,12 @@ SIGNATURES = {
     "gf_precond_get": (_I, [_P, _PI, _PI, _PD]),
     "gf_solve_opts_default": (None, [C.POINTER(gf_solve_opts)]),
     "gf_gmres_solve": (_I, [_P, _P, _P, _P, _P, C.POINTER(gf_solve_opts),
+                            C.POINTER(gf_solve_stats), _P]),
+    "gf_batch_create": (_I, [_I, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]),
+    "gf_batch_destroy": (_I, [_P]),
+    "gf_batch_assemble": (_I, [_P, _P]),
+    "gf_batch_factor": (_I, [_P, _P]),
+    "gf_batch_solve": (_I, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(gf_solve_opts),
                             C.POINTER(gf_solve_stats), _P]),
 }
 

@@ -165,6 +165,10 @@ class ElementAssembler:
     def set_variables(self, vec: DeviceVec):
         check(L.lib().gf_set_variables(self.h, vec.getPtr(), _stream()), "set_variables")
 
+    def set_thickness(self, thick: torch.Tensor):
+        """Per-element thickness (natural element order) on the device."""
+        check(L.lib().gf_assembler_set_thickness(self.h, _ptr(thick), _stream()), "set_thickness")
+
     def add_residual(self, res: DeviceVec, add=False, fuse_bcs=False):
         flags = (L.GF_ASSEMBLE_ADD if add else 0) | (L.GF_ASSEMBLE_FUSE_BCS if fuse_bcs else 0)
         check(L.lib().gf_add_residual(self.h, res.getPtr(), flags, _stream()), "add_residual")

@@ -1,0 +1,153 @@
+"""Batched uneven shell solves and the fill-level autotuner.
+
+A batch holds many independent plate / panel problems. Per problem the mesh,
+BSR pattern, coloured scatter schedule and ILU(k) symbolic data stay
+device-resident; a step re-assembles K (fused BCs) for every problem,
+refactors all preconditioners in one level-ordered launch and solves all
+problems together (gf_batch_*): one SpMV launch and one launch per
+triangular sweep for the whole batch, per-problem GMRES states. Precision:
+FP64, or FP32 ILU + FP32 SpMV inside FP64 iterative refinement (mixed).
+
+Autotuner: block ILU(0) is unstable on thin shells (Schur complements of the
+membrane-dominated rows lose definiteness), so the fill level k of the
+symbolic ILU(k) (computeILUk, include/linalg/bsr_utils.h:678-807) is chosen
+per problem: every candidate k is tried on the whole batch in one batched
+FP64 solve with an iteration cap, and each problem keeps the converging k
+with the smallest estimated sweep work (iterations x triangular levels).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from .assembler import BsrMat, ElementAssembler, ILUk_Preconditioner, SolveOptions, _stream
+
+FILL_CANDIDATES = (0, 1, 2, 3, 4, 6, 8, 12, 16, 24)
+
+
+class Batch:
+    """gf_batch handle over lists of assemblers, matrices, preconditioners."""
+
+    def __init__(self, asms, mats, pcs):
+        n = len(asms)
+        self.keep = (asms, mats, pcs)
+        A = (C.c_void_p * n)(*[a.h.value for a in asms])
+        K = (C.c_void_p * n)(*[m.h.value for m in mats])
+        P = (C.c_void_p * n)(*[p.h.value for p in pcs])
+        h = C.c_void_p()
+        L.check(L.lib().gf_batch_create(n, A, K, P, C.byref(h)), "gf_batch_create")
+        self.h = h
+        self.n = n
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h is not None and L._LIB is not None:
+            L.lib().gf_batch_destroy(h)
+            self.h = None
+
+    def assemble(self):
+        L.check(L.lib().gf_batch_assemble(self.h, _stream()), "gf_batch_assemble")
+
+    def factor(self):
+        L.check(L.lib().gf_batch_factor(self.h, _stream()), "gf_batch_factor")
+
+    def solve(self, bs, xs, opts):
+        n = self.n
+        B = (C.c_void_p * n)(*[b.data_ptr() for b in bs])
+        X = (C.c_void_p * n)(*[x.data_ptr() for x in xs])
+        stats = (L.gf_solve_stats * n)()
+        st = L.lib().gf_batch_solve(self.h, B, X, C.byref(opts), stats, _stream())
+        if st not in (L.GF_OK, L.GF_NOT_CONVERGED):
+            L.check(st, "gf_batch_solve")
+        return st, [{"iterations": s.iterations, "restarts": s.restarts,
+                     "refinements": s.refinements, "status": s.status,
+                     "rel_residual": s.rel_residual} for s in stats]
+
+
+def solve_opts(rtol=1e-8, mixed=False, restart=100, max_iters=20000, inner_rtol=1e-4):
+    return SolveOptions(restart=restart, max_iters=max_iters, rtol=rtol, side=1,
+                        mixed=1 if mixed else 0, inner_rtol=inner_rtol, max_refine=30,
+                        check_every=25)
+
+
+class BatchSolver:
+    """Problems resident on the current device, solved as one batch."""
+
+    def __init__(self, meshes, ordering="rcm", tune=True, fill=None, rtol=1e-8, restart=100):
+        self.rtol, self.restart = rtol, restart
+        self.meshes = meshes
+        self.asms = [ElementAssembler.from_mesh(m, ordering=ordering) for m in meshes]
+        self.mats = [BsrMat(a) for a in self.asms]
+        self.bs = [torch.tensor(m.loads, device="cuda") for m in meshes]
+        self.xs = [torch.zeros_like(b) for b in self.bs]
+        for a, k in zip(self.asms, self.mats):
+            a.add_jacobian(None, k, fuse_bcs=True)
+        n = len(meshes)
+        if fill is not None:
+            self.fills = [fill] * n if np.isscalar(fill) else list(fill)
+            self.tune_log = None
+        elif tune:
+            self.fills, self.tune_log = self._autotune()
+        else:
+            self.fills, self.tune_log = [0] * n, None
+        self.P64 = [ILUk_Preconditioner(a, k, "fp64") for a, k in zip(self.asms, self.fills)]
+        self.P32 = [ILUk_Preconditioner(a, k, "fp32") for a, k in zip(self.asms, self.fills)]
+        self.b64 = Batch(self.asms, self.mats, self.P64)
+        self.b32 = Batch(self.asms, self.mats, self.P32)
+        torch.cuda.synchronize()
+
+    def _autotune(self, cap=400):
+        n = len(self.meshes)
+        best = [None] * n
+        log = []
+        for k in FILL_CANDIDATES:
+            todo = [i for i in range(n) if best[i] is None or k <= best[i][2] + 4]
+            if not todo:
+                break
+            P = [ILUk_Preconditioner(self.asms[i], k, "fp64") for i in todo]
+            bt = Batch([self.asms[i] for i in todo], [self.mats[i] for i in todo], P)
+            try:
+                bt.factor()
+            except L.GpuFemError:
+                log.append((k, "factor failed"))
+                continue
+            for i in todo:
+                self.xs[i].zero_()
+            st, stats = bt.solve([self.bs[i] for i in todo], [self.xs[i] for i in todo],
+                                 solve_opts(self.rtol, False, restart=200, max_iters=cap))
+            for j, i in enumerate(todo):
+                s = stats[j]
+                nlev = P[j].info()["levels_L"] + P[j].info()["levels_U"]
+                ok = s["status"] == L.GF_OK
+                log.append((i, k, s["iterations"], s["rel_residual"], nlev, ok))
+                if ok:
+                    cost = s["iterations"] * nlev
+                    if best[i] is None or cost < best[i][0]:
+                        best[i] = (cost, k, k)
+            if all(b is not None for b in best) and k >= max(b[1] for b in best) + 4:
+                break
+        missing = [self.meshes[i].name for i in range(n) if best[i] is None]
+        if missing:
+            raise RuntimeError(f"no ILU fill level converged for {missing}")
+        return [b[1] for b in best], log
+
+    def step(self, mixed: bool, host_io=None):
+        """Assemble, factor and solve every problem once."""
+        if host_io is not None:
+            for b, hb in zip(self.bs, host_io[0]):
+                b.copy_(hb, non_blocking=True)
+        bt = self.b32 if mixed else self.b64
+        bt.assemble()
+        bt.factor()
+        for x in self.xs:
+            x.zero_()
+        st, stats = bt.solve(self.bs, self.xs, solve_opts(self.rtol, mixed, self.restart))
+        if st != L.GF_OK:
+            raise RuntimeError(f"batch solve failed: {[s for s in stats if s['status']]}")
+        if host_io is not None:
+            for x, hx in zip(self.xs, host_io[1]):
+                hx.copy_(x, non_blocking=True)
+        return stats

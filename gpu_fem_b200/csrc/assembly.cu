@@ -5,13 +5,15 @@
 // scatter with FP64 atomicAdd (include/linalg/vec.h:278-293,
 // include/linalg/bsr_mat.h:229-276).
 //
-// Here one warp owns one element:
-//   * node coordinates and DOFs are gathered once into the warp's shared
-//     memory slot, the per-element geometry (normals, nodal frames, the four
-//     quadrature-point frames, the tying-point vectors) is spread over lanes;
-//   * lane l < 24 builds column l of the four 9x24 strain matrices B_q and
-//     keeps D B_q[:, l] in registers; column l of K_e = sum_q B_q^T D B_q is
-//     a 36-term product against the shared B (broadcast reads);
+// Here a warp works on batches of up to eight elements:
+//   * coordinates and DOFs of the batch are gathered into the warp's shared
+//     memory slot and the per-element geometry (normals, nodal frames, the
+//     four quadrature-point frames, the tying-point vectors) is computed by
+//     8 x 4 lanes at once;
+//   * per element, lane l < 24 builds column l of the four 9x24 strain
+//     matrices B_q and of D B_q; each of the 32 lanes then owns a 3x6 tile of
+//     K_e = sum_q B_q^T D B_q (144 contiguous bytes of one 6x6 BSR block) and
+//     writes it with 16-byte stores; R_e = K_e u_e follows from the tiles;
 //   * the scatter follows the coloured schedule built on the host: one CTA
 //     per chunk, chunks of one colour per launch, element colours separated
 //     by __syncthreads(). The first toucher of a block stores, later touchers
@@ -24,12 +26,15 @@
 namespace gf {
 
 constexpr int kAsmWarps = 4;
+constexpr int kEPW = 8;          // elements per warp batch (geometry spread over 8 x 4 lanes)
+constexpr int kChunkSize = 128;  // elements per chunk (one CTA per chunk)
 
 struct WarpSlot {
-  double X[12];
-  double U[24];
-  ElemGeom g;
-  double Bt[36][24];
+  double X[kEPW][12];
+  double U[kEPW][24];
+  ElemGeom g[kEPW];
+  double Bt[36][24];   // B_q[k][l] of the current element, row qk = 9q + k
+  double DBt[36][24];  // (D B_q)[k][l]
   double E[36];
   double S[36];
 };
@@ -55,121 +60,173 @@ struct AsmParams {
 
 enum { MODE_JAC = 0, MODE_RES = 1, MODE_ENERGY = 2 };
 
+// Geometry of up to kEPW elements (schedule positions s0 .. s0+cnt-1).
+__device__ void batch_geometry(int s0, int cnt, WarpSlot& w, const AsmParams& P, int lane) {
+  for (int t = lane; t < cnt * 12; t += 32) {
+    const int k = t / 12, i = t % 12;
+    const int node = P.sconn[4 * (s0 + k) + i / 3];
+    w.X[k][i] = P.xpts[3 * node + i % 3];
+  }
+  for (int t = lane; t < cnt * 24; t += 32) {
+    const int k = t / 24, i = t % 24;
+    const int node = P.sconn[4 * (s0 + k) + i / 6];
+    w.U[k][i] = P.vars ? P.vars[6 * node + i % 6] : 0.0;
+  }
+  __syncwarp();
+  const int k = lane >> 2, n = lane & 3;
+  const bool on = k < cnt;
+  Material m;
+  if (on) m = P.mats[P.smat ? P.smat[s0 + k] : 0];
+  if (on) geom_normal(w.X[k], n, &w.g[k].fn[3 * n]);
+  __syncwarp();
+  if (on) {
+    geom_node(m, w.X[k], w.g[k].fn, n, w.g[k].Tn01[n], w.g[k].XTn[n], w.g[k].tcross[n]);
+    geom_quad(m, w.X[k], w.g[k].fn, n, w.g[k].T[n], w.g[k].A[n], w.g[k].Az[n],
+              w.g[k].scale[n]);
+  }
+  for (int t = lane; t < cnt * 5; t += 32) geom_tying(w.X[t / 5], w.g[t / 5].fn, t % 5, w.g[t / 5]);
+  __syncwarp();
+}
+
 template <int MODE>
-__device__ void process_element(int s, WarpSlot& w, const AsmParams& P, int lane,
+__device__ void process_element(int s, int k, WarpSlot& w, const AsmParams& P, int lane,
                                 double& energy_acc) {
-  const int4 cn = reinterpret_cast<const int4*>(P.sconn)[s];
-  const int nodes[4] = {cn.x, cn.y, cn.z, cn.w};
-  if (lane < 12) w.X[lane] = P.xpts[3 * nodes[lane / 3] + lane % 3];
-  if (lane < 24) w.U[lane] = P.vars ? P.vars[6 * nodes[lane / 6] + lane % 6] : 0.0;
   const Material m = P.mats[P.smat ? P.smat[s] : 0];
   const double t = P.sthick[s];
-  __syncwarp();
-  if (lane < 4) geom_normal(w.X, lane, &w.g.fn[3 * lane]);
-  __syncwarp();
-  if (lane < 4) {
-    geom_node(m, w.X, w.g.fn, lane, w.g.Tn01[lane], w.g.XTn[lane], w.g.tcross[lane]);
-  } else if (lane < 8) {
-    const int q = lane - 4;
-    geom_quad(m, w.X, w.g.fn, q, w.g.T[q], w.g.A[q], w.g.Az[q], w.g.scale[q]);
-  } else if (lane < 13) {
-    geom_tying(w.X, w.g.fn, lane - 8, w.g);
-  }
-  __syncwarp();
-  double Bc[36];
+  const ElemGeom& g = w.g[k];
   if (lane < 24) {
-    bmat_column(w.g, lane, Bc);
+    double Bc[36];
+    bmat_column(g, lane, Bc);
 #pragma unroll
-    for (int k = 0; k < 36; k++) w.Bt[k][lane] = Bc[k];
-  }
-  __syncwarp();
-
-  const bool fuse = (P.flags & GF_ASSEMBLE_FUSE_BCS) != 0;
-  const bool add = (P.flags & GF_ASSEMBLE_ADD) != 0;
-  const uint32_t ft = P.sft[s];
-  uint32_t bcm[4] = {0, 0, 0, 0};
-  if (fuse)
-    for (int a = 0; a < 4; a++) bcm[a] = P.bcmask[nodes[a]];
-
-  double rj = 0.0;  // residual entry of DOF `lane`
-  if (MODE == MODE_JAC) {
-    if (lane < 24) {
-      // D B_q[:, lane] in place
+    for (int qk = 0; qk < 36; qk++) w.Bt[qk][lane] = Bc[qk];
+    if (MODE == MODE_JAC) {
 #pragma unroll
       for (int q = 0; q < 4; q++) {
         double Sq[9];
-        stress(m, t, w.g.scale[q], &Bc[9 * q], Sq);
+        stress(m, t, g.scale[q], &Bc[9 * q], Sq);
 #pragma unroll
-        for (int k = 0; k < 9; k++) Bc[9 * q + k] = Sq[k];
+        for (int kk = 0; kk < 9; kk++) w.DBt[9 * q + kk][lane] = Sq[kk];
       }
-      double acc[24];
+    }
+  }
+  __syncwarp();
+  const int4 cn = reinterpret_cast<const int4*>(P.sconn)[s];
+  const int nodes[4] = {cn.x, cn.y, cn.z, cn.w};
+  const bool fuse = (P.flags & GF_ASSEMBLE_FUSE_BCS) != 0;
+  const bool add = (P.flags & GF_ASSEMBLE_ADD) != 0;
+  const uint32_t ft = P.sft[s];
+
+  if (MODE == MODE_JAC) {
+    // lane (I, J): rows 3I..3I+2, columns 6J..6J+5 of K_e (one block row slice)
+    const int I = lane >> 2, J = lane & 3;
+    double acc[3][6];
 #pragma unroll
-      for (int i = 0; i < 24; i++) acc[i] = 0.0;
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+      for (int c = 0; c < 6; c++) acc[r][c] = 0.0;
 #pragma unroll 4
-      for (int qk = 0; qk < 36; qk++) {
-        const double d = Bc[qk];
-        const double2* row = reinterpret_cast<const double2*>(&w.Bt[qk][0]);
+    for (int qk = 0; qk < 36; qk++) {
+      const double b0 = w.Bt[qk][3 * I], b1 = w.Bt[qk][3 * I + 1], b2 = w.Bt[qk][3 * I + 2];
+      const double2* dp = reinterpret_cast<const double2*>(&w.DBt[qk][6 * J]);
+      const double2 d01 = dp[0], d23 = dp[1], d45 = dp[2];
+      const double d[6] = {d01.x, d01.y, d23.x, d23.y, d45.x, d45.y};
 #pragma unroll
-        for (int i = 0; i < 12; i++) {
-          const double2 b = row[i];
-          acc[2 * i] = fma(b.x, d, acc[2 * i]);
-          acc[2 * i + 1] = fma(b.y, d, acc[2 * i + 1]);
+      for (int c = 0; c < 6; c++) {
+        acc[0][c] = fma(b0, d[c], acc[0][c]);
+        acc[1][c] = fma(b1, d[c], acc[1][c]);
+        acc[2][c] = fma(b2, d[c], acc[2][c]);
+      }
+    }
+    const int a = I >> 1, r0 = 3 * (I & 1), b = J;
+    // residual part for rows 3I..3I+2 over columns of node b
+    double rp[3];
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+      double s_ = 0.0;
+#pragma unroll
+      for (int c = 0; c < 6; c++) s_ = fma(acc[r][c], w.U[k][6 * b + c], s_);
+      rp[r] = s_;
+    }
+    if (P.values) {
+      const uint32_t bca = fuse ? P.bcmask[nodes[a]] : 0u;
+      const uint32_t bcb = fuse ? P.bcmask[nodes[b]] : 0u;
+      const bool first = (ft >> (4 * a + b)) & 1;
+      const int blk = P.semap[16 * s + 4 * a + b];
+      double* dst = P.values + 36 * (size_t)blk + 6 * r0;
+      double v[18];
+#pragma unroll
+      for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int c = 0; c < 6; c++) {
+          double x = acc[r][c];
+          if (fuse && (((bca >> (r0 + r)) & 1) || ((bcb >> c) & 1)))
+            x = (a == b && r0 + r == c && first) ? 1.0 : 0.0;
+          v[6 * r + c] = x;
+        }
+      double2* d2 = reinterpret_cast<double2*>(dst);
+      if (first && !add) {
+#pragma unroll
+        for (int h = 0; h < 9; h++) d2[h] = make_double2(v[2 * h], v[2 * h + 1]);
+      } else {
+#pragma unroll
+        for (int h = 0; h < 9; h++) {
+          const double2 o = d2[h];
+          d2[h] = make_double2(o.x + v[2 * h], o.y + v[2 * h + 1]);
         }
       }
-      // acc[i] = K[i][lane] = K[lane][i]
+    }
+    // R rows 3I..3I+2: sum the four column slices (lanes J = 0..3 of row group I)
 #pragma unroll
-      for (int i = 0; i < 24; i++) rj = fma(acc[i], w.U[i], rj);
-      if (P.values) {
-        const int b = lane / 6, c = lane % 6;
-        const bool cbc = (bcm[b] >> c) & 1;
-#pragma unroll
-        for (int a = 0; a < 4; a++) {
-          const int blk = P.semap[16 * s + 4 * a + b];
-          double* dst = P.values + 36 * (size_t)blk + c;
-          const bool first = (ft >> (4 * a + b)) & 1;
-#pragma unroll
-          for (int r = 0; r < 6; r++) {
-            double v = acc[6 * a + r];
-            if (fuse && (cbc || ((bcm[a] >> r) & 1))) v = (a == b && r == c && first) ? 1.0 : 0.0;
-            if (first && !add)
-              dst[6 * r] = v;
-            else
-              dst[6 * r] += v;
-          }
-        }
-      }
+    for (int r = 0; r < 3; r++) {
+      rp[r] += __shfl_xor_sync(0xffffffffu, rp[r], 1);
+      rp[r] += __shfl_xor_sync(0xffffffffu, rp[r], 2);
+    }
+    if (P.res && J < 3) {
+      const int r = r0 + J;  // lanes J = 0,1,2 store rows r0, r0+1, r0+2
+      double val = rp[J == 0 ? 0 : (J == 1 ? 1 : 2)];
+      if (fuse && ((P.bcmask[nodes[a]] >> r) & 1)) val = 0.0;
+      double* dst = P.res + 6 * (size_t)nodes[a] + r;
+      const bool first = (ft >> (16 + a)) & 1;
+      if (first && !add)
+        *dst = val;
+      else
+        *dst += val;
     }
   } else {
-    // E_q = B_q u (36 entries over 32 lanes), S_q = D E_q, R = sum_q B_q^T S_q
-    for (int k = lane; k < 36; k += 32) {
-      double e = 0.0;
+    // E_q = B_q u, S_q = D E_q, R = sum_q B_q^T S_q
+    double e0 = 0.0, e1 = 0.0;
 #pragma unroll
-      for (int l = 0; l < 24; l++) e = fma(w.Bt[k][l], w.U[l], e);
-      w.E[k] = e;
+    for (int l = 0; l < 24; l++) {
+      e0 = fma(w.Bt[lane][l], w.U[k][l], e0);
+      if (lane < 4) e1 = fma(w.Bt[32 + lane][l], w.U[k][l], e1);
     }
+    double* E = w.E;
+    E[lane] = e0;
+    if (lane < 4) E[32 + lane] = e1;
     __syncwarp();
-    if (lane < 4) stress(m, t, w.g.scale[lane], &w.E[9 * lane], &w.S[9 * lane]);
+    if (lane < 4) stress(m, t, g.scale[lane], &E[9 * lane], &w.S[9 * lane]);
     __syncwarp();
     if (MODE == MODE_ENERGY) {
       if (lane == 0) {
         double U = 0.0;
-        for (int k = 0; k < 36; k++) U += 0.5 * w.E[k] * w.S[k];
+        for (int q = 0; q < 36; q++) U += 0.5 * E[q] * w.S[q];
         energy_acc += U;
       }
     } else if (lane < 24) {
+      double rj = 0.0;
 #pragma unroll
-      for (int k = 0; k < 36; k++) rj = fma(w.Bt[k][lane], w.S[k], rj);
+      for (int qk = 0; qk < 36; qk++) rj = fma(w.Bt[qk][lane], w.S[qk], rj);
+      if (P.res) {
+        const int b = lane / 6, c = lane % 6;
+        if (fuse && ((P.bcmask[nodes[b]] >> c) & 1)) rj = 0.0;
+        double* dst = P.res + 6 * (size_t)nodes[b] + c;
+        const bool first = (ft >> (16 + b)) & 1;
+        if (first && !add)
+          *dst = rj;
+        else
+          *dst += rj;
+      }
     }
-  }
-  if (MODE != MODE_ENERGY && P.res && lane < 24) {
-    const int b = lane / 6, c = lane % 6;
-    if (fuse && ((bcm[b] >> c) & 1)) rj = 0.0;
-    double* dst = P.res + 6 * (size_t)nodes[b] + c;
-    const bool first = (ft >> (16 + b)) & 1;
-    if (first && !add)
-      *dst = rj;
-    else
-      *dst += rj;
   }
   __syncwarp();
 }
@@ -184,11 +241,15 @@ __global__ void __launch_bounds__(kAsmWarps * 32)
   const int s0 = P.chunk_start[li];
   const int32_t* off = &P.ec_off[(size_t)li * (kMaxEC + 1)];
   double energy_acc = 0.0;
+  WarpSlot& w = slots[warp];
   for (int col = 0; col < kMaxEC; col++) {
     const int b = off[col], e = off[col + 1];
     if (b == e) continue;
-    for (int k = b + warp; k < e; k += kAsmWarps)
-      process_element<MODE>(s0 + k, slots[warp], P, lane, energy_acc);
+    for (int base = b + warp * kEPW; base < e; base += kAsmWarps * kEPW) {
+      const int cnt = min(kEPW, e - base);
+      batch_geometry(s0 + base, cnt, w, P, lane);
+      for (int k = 0; k < cnt; k++) process_element<MODE>(s0 + base + k, k, w, P, lane, energy_acc);
+    }
     __syncthreads();
   }
   if (MODE == MODE_ENERGY) {
@@ -197,7 +258,7 @@ __global__ void __launch_bounds__(kAsmWarps * 32)
     __syncthreads();
     if (threadIdx.x == 0) {
       double sum = 0.0;
-      for (int w = 0; w < kAsmWarps; w++) sum += part[w];
+      for (int w2 = 0; w2 < kAsmWarps; w2++) sum += part[w2];
       P.energy_part[li] = sum;
     }
   }
@@ -232,6 +293,11 @@ __global__ void bc_mat_kernel(const int32_t* entries, int n, const int32_t* cols
     const int r = is_col ? k : inner, c = is_col ? inner : k;
     v[6 * r + c] = (6 * brow + r == 6 * bcol + c) ? 1.0 : 0.0;
   }
+}
+
+__global__ void gather_thickness(const int32_t* order, int n, const double* in, double* out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) out[t] = in[order[t]];
 }
 
 __global__ void bc_vec_kernel(const int32_t* bcs, int n, double* vec) {
@@ -281,7 +347,7 @@ static gf_status launch_assembly(gf_assembler* a, double* values, double* res, i
     const int nblk = s.cc_start[cc + 1] - s.cc_start[cc];
     if (nblk == 0) continue;
     P.chunk_base = s.cc_start[cc];
-    assemble_kernel<MODE><<<nblk, kAsmWarps * 32, smem, st>>>(P);
+    assemble_kernel<MODE><<<nblk, kAsmWarps * 32, smem, st>>>(P); ::gf::count_launch();
     GF_CHECK_LAUNCH();
   }
   return GF_OK;
@@ -328,7 +394,7 @@ gf_status gf_assembler_create(const gf_mesh_desc* d, gf_assembler** out) {
   for (int i = 0; i < nn; i++) a->iperm[a->perm[i]] = i;
   a->pat = permute_pattern(a->pat0, a->perm);
   elem_ind_map(ne, d->conn, a->pat, a->perm, a->emap);
-  if (build_schedule(ne, nn, d->conn, a->emap, a->pat.nnz(), 32, a->sched) != 0) {
+  if (build_schedule(ne, nn, d->conn, a->emap, a->pat.nnz(), kChunkSize, a->sched) != 0) {
     delete a;
     return GF_INVALID_ARG;
   }
@@ -409,6 +475,7 @@ gf_status gf_assembler_create(const gf_mesh_desc* d, gf_assembler** out) {
   up(a->d_smat.upload(smat));
   up(a->d_sft.upload(sft));
   up(a->d_sthick.upload(sthick));
+  up(a->d_sorder.upload(s.order));
   up(a->d_chunk_start.upload(s.chunk_start));
   up(a->d_ec_off.upload(s.ec_off));
   up(a->d_mats.upload(a->mats));
@@ -484,7 +551,7 @@ gf_status gf_add_energy(gf_assembler* a, double* h_energy, void* stream) {
   gf_status s = launch_assembly<MODE_ENERGY>(a, nullptr, nullptr, 0, st);
   if (s != GF_OK) return s;
   sum_kernel<<<1, 256, 0, st>>>(a->d_energy_part.p, a->sched.nchunks,
-                                a->d_energy_part.p + a->sched.nchunks);
+                                a->d_energy_part.p + a->sched.nchunks); ::gf::count_launch();
   GF_CHECK_LAUNCH();
   GF_CUDA(cudaMemcpyAsync(h_energy, a->d_energy_part.p + a->sched.nchunks, sizeof(double),
                           cudaMemcpyDeviceToHost, st));
@@ -492,11 +559,19 @@ gf_status gf_add_energy(gf_assembler* a, double* h_energy, void* stream) {
   return GF_OK;
 }
 
+gf_status gf_assembler_set_thickness(gf_assembler* a, const double* d_thick, void* stream) {
+  if (!a || !d_thick) return GF_INVALID_ARG;
+  gather_thickness<<<(a->nelem + 255) / 256, 256, 0, as_stream(stream)>>>(
+      a->d_sorder.p, a->nelem, d_thick, a->d_sthick.p); ::gf::count_launch();
+  GF_CHECK_LAUNCH();
+  return GF_OK;
+}
+
 gf_status gf_apply_bcs_vec(gf_assembler* a, double* d_vec, void* stream) {
   if (!a || !d_vec) return GF_INVALID_ARG;
   if (a->nbcs == 0) return GF_OK;
   bc_vec_kernel<<<(a->nbcs + 255) / 256, 256, 0, as_stream(stream)>>>(a->d_bcs.p, a->nbcs,
-                                                                      d_vec);
+                                                                      d_vec); ::gf::count_launch();
   GF_CHECK_LAUNCH();
   return GF_OK;
 }
@@ -505,7 +580,7 @@ gf_status gf_apply_bcs_mat(gf_assembler* a, gf_bsr* mat, void* stream) {
   if (!a || !mat || mat->a != a) return GF_INVALID_ARG;
   if (a->nbc_entries == 0) return GF_OK;
   bc_mat_kernel<<<(a->nbc_entries + 127) / 128, 128, 0, as_stream(stream)>>>(
-      a->d_bc_entries.p, a->nbc_entries, a->d_cols.p, mat->vals.p);
+      a->d_bc_entries.p, a->nbc_entries, a->d_cols.p, mat->vals.p); ::gf::count_launch();
   GF_CHECK_LAUNCH();
   return GF_OK;
 }
@@ -543,7 +618,7 @@ gf_status gf_permute_vec(gf_assembler* a, const double* d_in, double* d_out, int
   if (!a || !d_in || !d_out || d_in == d_out || (dir != 0 && dir != 1)) return GF_INVALID_ARG;
   const int n = 6 * a->nnodes;
   permute_kernel<<<(n + 255) / 256, 256, 0, as_stream(stream)>>>(a->d_perm.p, a->nnodes, d_in,
-                                                                  d_out, dir);
+                                                                  d_out, dir); ::gf::count_launch();
   GF_CHECK_LAUNCH();
   return GF_OK;
 }

@@ -1,4 +1,5 @@
 // Library-level C ABI: status strings, version, last-error text.
+#include <atomic>
 #include <cstdio>
 #include <string>
 
@@ -9,9 +10,13 @@ static thread_local std::string g_last_error;
 void set_last_error(const char* where, cudaError_t e) {
   g_last_error = std::string(where) + ": " + cudaGetErrorString(e);
 }
+static std::atomic<long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 }  // namespace gf
 
 extern "C" {
+
+long long gf_launch_count(void) { return gf::g_launches.load(); }
 
 const char* gf_status_string(gf_status s) {
   switch (s) {

@@ -13,6 +13,8 @@ namespace gf {
 
 // Thread-local text of the last CUDA error seen by the library.
 void set_last_error(const char* where, cudaError_t e);
+// Process-wide count of kernels this library has launched.
+void count_launch();
 
 #define GF_CUDA(call)                                  \
   do {                                                 \
@@ -98,6 +100,23 @@ struct Schedule {
   std::vector<int32_t> ec_off;        // [nchunks * (kMaxEC+1)] colour offsets within chunk
 };
 constexpr int kMaxEC = 15;
+
+// Per-problem descriptor used by the batched solver kernels: block rows,
+// offset of the problem in the batch vector space (in block rows), the
+// matrix pattern and values (FP64 and the FP32 copy of the mixed mode), and
+// the ILU pattern and factor values.
+struct ProbDev {
+  int n, off;
+  const int32_t* rowp;
+  const int32_t* cols;
+  const double* A64;
+  const float* A32;
+  const int32_t* prowp;
+  const int32_t* pcols;
+  const int32_t* pdiag;
+  double* LU64;
+  float* LU32;
+};
 int build_schedule(int nelem, int nnodes, const int32_t* conn, const std::vector<int32_t>& emap,
                    int nnzb, int chunk_size, Schedule& s);
 
@@ -122,6 +141,7 @@ struct gf_assembler {
   gf::DevBuf<int32_t> d_sconn, d_semap, d_smat;
   gf::DevBuf<uint32_t> d_sft;
   gf::DevBuf<double> d_sthick;
+  gf::DevBuf<int32_t> d_sorder;     // schedule position -> element
   gf::DevBuf<int32_t> d_chunk_list, d_chunk_start, d_ec_off;
   gf::DevBuf<gf::Material> d_mats;
   // device: pattern (solver order) and BC entry list
@@ -135,4 +155,7 @@ struct gf_assembler {
 struct gf_bsr {
   gf_assembler* a = nullptr;
   gf::DevBuf<double> vals;
+  gf::DevBuf<float> vals32;           // FP32 copy for the mixed-precision SpMV
+  gf::DevBuf<gf::ProbDev> desc;       // one-entry table for gf_bsr_spmv
+  gf::DevBuf<int32_t> rowprob;
 };

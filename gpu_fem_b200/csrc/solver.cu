@@ -1,54 +1,119 @@
-// BSR SpMV, block ILU(k) numeric factorization, level-ordered triangular
-// solves and the device-resident GMRES / iterative-refinement driver.
+// Batched solver engine: BSR SpMV, block ILU(k) factorization, block
+// triangular sweeps and restarted GMRES / iterative refinement over a batch
+// of independent problems (a single problem is a batch of one).
 //
 // Reference: cusparseDbsrmv, cusparseDbsrilu02 and cusparseDbsrsv2_solve as
-// called by examples/iterative/gmres.cu:374-771, and the GMRES loop there.
+// called by examples/iterative/gmres.cu:374-771, and the GMRES loop there
+// (left-preconditioned GMRES(m), MGS, host Givens; bugs fixed: dot length
+// nvars, m+1 basis vectors, restarts).
 //
-// Triangular dependencies (factorization and both solves) are handled in
-// one persistent launch per sweep: warps take rows in level order from an
-// atomic counter and wait on per-row ready flags of the rows they depend on.
-// Every row a warp waits for was taken earlier by a running warp, so the
-// sweep cannot deadlock; every wait is bounded (kSpinLimit polls) and a wait
-// that runs out sets an error bit in the status word instead of hanging.
-// Flags carry an epoch read from device memory, so the same launch
-// sequence can be captured in a CUDA graph and replayed.
+// Batch layout: every problem keeps its own pattern / values / factor
+// buffers; a device table of ProbDev descriptors gives each kernel the
+// problem of a global block row (row_prob) and its offset in the batch vector
+// space. Triangular work (factorization, L and U sweeps) runs as one
+// persistent launch per sweep over the merged level order of all problems:
+// warps take rows from an atomic counter in that order, so every row a warp
+// waits for was taken earlier by a running warp and a sweep cannot deadlock.
+//  * factorization: per-row ready flags carrying an epoch;
+//  * sweeps: the output vector is pre-filled with a signalling-NaN sentinel
+//    that arithmetic never produces; a consumer polls the producer's six
+//    values directly (one L2 round trip, no flag or fence on the path).
+// Every wait is bounded (2 s of %globaltimer); a wait that runs out sets an
+// error bit in the status word and the launch ends instead of hanging.
+//
+// GMRES reductions are segmented per problem over fixed 4096-entry chunks
+// aligned to each problem's own vector, with per-problem Arnoldi states, so
+// a problem's iterates are bitwise identical alone and inside any batch.
 #include <algorithm>
+#include <array>
+#include <chrono>
 #include <cmath>
-#include <cstdio>
+#include <cstring>
+#include <numeric>
 
 #include "gf_internal.h"
 
 namespace gf {
 
-constexpr long long kSpinLimit = 1ll << 26;
+constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s per wait
 enum { ST_TIMEOUT = 1, ST_ZERO_PIVOT = 2, ST_NAN = 4 };
+constexpr unsigned long long kSentinel = 0x7FF4DEADBEEF0000ull;  // signalling-NaN payload
+constexpr int kChunk = 4096;
+constexpr int kRedThreads = 256;
 
 struct SweepCtl {
-  int epoch;     // incremented before every sweep
-  int counter;   // work counter, reset with the epoch
-  int status;    // error bits
-  int pivot;     // first zero-pivot row + 1
+  int epoch;
+  int counter;
+  int status;
+  int pivot;
 };
 
+__device__ __forceinline__ bool is_sentinel(double v) {
+  return (unsigned long long)__double_as_longlong(v) == kSentinel;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Coherent (gpu-scope) load of a value another SM may be writing.
+__device__ __forceinline__ double ld_relaxed(const double* p) {
+  double v;
+  asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed(double* p, double v) {
+  asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+}
+// Bounded-wait helper: true once more than kWaitLimitNs has passed since t0.
+__device__ __forceinline__ bool wait_expired(unsigned long long t0, unsigned& polls) {
+  if ((++polls & 63u) != 0u) return false;
+  return global_ns() - t0 > kWaitLimitNs;
+}
+__device__ __forceinline__ int ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(int* p, int v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__global__ void sweep_begin(SweepCtl* c) {
+  c->epoch += 1;
+  c->counter = 0;
+}
+__global__ void fill_sentinel(double* v, size_t n) {
+  const double s = __longlong_as_double((long long)kSentinel);
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += (size_t)gridDim.x * blockDim.x)
+    v[t] = s;
+}
+
 // ------------------------------------------------------------------ SpMV
-// y = alpha A x + beta y. One warp per block row; 4 groups of 6 lanes, lane
-// (g, r) handles row r of block 4k+g; 6-lane groups are reduced with two
-// shuffles.
+// y = alpha A x + beta y over all rows of live problems; one warp per block
+// row, 4 groups of 6 lanes (group g takes blocks g, g+4, ...).
 template <class VT>
-__global__ void spmv_kernel(int n, const int32_t* __restrict__ rowp,
-                            const int32_t* __restrict__ cols, const VT* __restrict__ A,
-                            const double* __restrict__ x, double alpha, double beta,
-                            double* __restrict__ y) {
+__global__ void bspmv_kernel(int nrows, const int32_t* __restrict__ row_prob,
+                             const ProbDev* __restrict__ P, const int* __restrict__ live,
+                             const double* __restrict__ x, double alpha, double beta,
+                             double* __restrict__ y) {
   const int lane = threadIdx.x & 31;
-  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (row >= n) return;
+  const int grow = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (grow >= nrows) return;
+  const int p = row_prob[grow];
+  if (live && !live[p]) return;
+  const ProbDev& d = P[p];
+  const int i = grow - d.off;
+  const VT* A = sizeof(VT) == 8 ? (const VT*)d.A64 : (const VT*)d.A32;
+  const double* xb = x + 6 * (size_t)d.off;
   const int g = lane / 6, r = lane % 6;
   double acc = 0.0;
   if (g < 4) {
-    const int b0 = rowp[row], b1 = rowp[row + 1];
+    const int b0 = d.rowp[i], b1 = d.rowp[i + 1];
     for (int blk = b0 + g; blk < b1; blk += 4) {
       const VT* a = A + 36 * (size_t)blk + 6 * r;
-      const double* xx = x + 6 * (size_t)cols[blk];
+      const double* xx = xb + 6 * (size_t)d.cols[blk];
 #pragma unroll
       for (int c = 0; c < 6; c++) acc = fma((double)a[c], xx[c], acc);
     }
@@ -56,49 +121,14 @@ __global__ void spmv_kernel(int n, const int32_t* __restrict__ rowp,
   acc += __shfl_down_sync(0xffffffffu, acc, 12);
   acc += __shfl_down_sync(0xffffffffu, acc, 6);
   if (lane < 6) {
-    double* yy = y + 6 * (size_t)row + lane;
+    double* yy = y + 6 * (size_t)grow + lane;
     *yy = (beta == 0.0) ? alpha * acc : alpha * acc + beta * (*yy);
   }
 }
 
-// ------------------------------------------------------------ sweep control
-__global__ void sweep_begin(SweepCtl* c) {
-  c->epoch += 1;
-  c->counter = 0;
-}
-
-__device__ __forceinline__ int fetch_row(SweepCtl* c, int lane) {
-  int idx = 0;
-  if (lane == 0) idx = atomicAdd(&c->counter, 1);
-  return __shfl_sync(0xffffffffu, idx, 0);
-}
-
-__device__ __forceinline__ void wait_flag(const int* flags, int k, int epoch, SweepCtl* c) {
-  long long spins = 0;
-  while (*((volatile const int*)&flags[k]) != epoch) {
-    if (++spins > kSpinLimit) {
-      atomicOr(&c->status, ST_TIMEOUT);
-      break;
-    }
-  }
-  __threadfence();
-}
-
-__device__ __forceinline__ void publish(int* flags, int i, int epoch, int lane) {
-  __threadfence();
-  __syncwarp();
-  if (lane == 0) *((volatile int*)&flags[i]) = epoch;
-}
-
 // ----------------------------------------------------- block ILU factorization
-// IKJ block ILU on the given pattern (FP64, in place). Lower blocks become
-// L_ik = A_ik U_kk^{-1}; the diagonal block is replaced by U_ii^{-1}.
 __device__ void inv6_warp(double* M, double* Inv, int lane, SweepCtl* ctl, int row) {
-  // Gauss-Jordan with partial pivoting on a 6x6 block held in shared memory;
-  // lane t < 36 owns one entry of the augmented right half via two passes.
-  if (lane < 32) {
-    for (int t = lane; t < 36; t += 32) Inv[t] = (t / 6 == t % 6) ? 1.0 : 0.0;
-  }
+  for (int t = lane; t < 36; t += 32) Inv[t] = (t / 6 == t % 6) ? 1.0 : 0.0;
   __syncwarp();
   for (int c = 0; c < 6; c++) {
     int p = c;
@@ -132,7 +162,6 @@ __device__ void inv6_warp(double* M, double* Inv, int lane, SweepCtl* ctl, int r
       dst[6 * c + lane % 6] *= piv;
     }
     __syncwarp();
-    // eliminate column c from other rows: lanes cover (row, col) of both halves
     double f[6];
     for (int r = 0; r < 6; r++) f[r] = M[6 * r + c];
     __syncwarp();
@@ -146,10 +175,12 @@ __device__ void inv6_warp(double* M, double* Inv, int lane, SweepCtl* ctl, int r
   }
 }
 
-__global__ void __launch_bounds__(128) ilu_factor_kernel(
-    int n, const int32_t* __restrict__ rowp, const int32_t* __restrict__ cols,
-    const int32_t* __restrict__ diag, const int32_t* __restrict__ order, double* LU, int* flags,
-    SweepCtl* ctl) {
+// IKJ block ILU on each problem's ILU pattern (FP64, in place): lower blocks
+// become L_ik = A_ik U_kk^{-1}, the diagonal block is replaced by U_ii^{-1}.
+__global__ void __launch_bounds__(128) bfactor_kernel(int nrows, const int32_t* __restrict__ row_prob,
+                                                      const ProbDev* __restrict__ P,
+                                                      const int32_t* __restrict__ order,
+                                                      int* flags, SweepCtl* ctl) {
   __shared__ double sm[4][3][36];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double* Lb = sm[warp][0];
@@ -157,27 +188,51 @@ __global__ void __launch_bounds__(128) ilu_factor_kernel(
   double* Inv = sm[warp][2];
   const int epoch = ctl->epoch;
   while (true) {
-    const int idx = fetch_row(ctl, lane);
-    if (idx >= n) break;
-    const int i = order[idx];
+    int idx = 0;
+    if (lane == 0) idx = atomicAdd(&ctl->counter, 1);
+    idx = __shfl_sync(0xffffffffu, idx, 0);
+    if (idx >= nrows) break;
+    const int grow = order[idx];
+    const int p = row_prob[grow];
+    const ProbDev& d = P[p];
+    const int i = grow - d.off;
+    const int32_t* rowp = d.prowp;
+    const int32_t* cols = d.pcols;
+    const int32_t* diag = d.pdiag;
+    double* LU = d.LU64;
     const int r0 = rowp[i], r1 = rowp[i + 1], di = diag[i];
+    // wait for every lower dependency, polled in parallel by the lanes
+    bool timed_out = false;
+    for (int base = r0; base < di; base += 32) {
+      const int kp = base + lane;
+      if (kp < di) {
+        const int* f = &flags[d.off + cols[kp]];
+        const unsigned long long t0 = global_ns();
+        unsigned polls = 0;
+        while (ld_acquire(f) != epoch) {
+          if (wait_expired(t0, polls)) {
+            timed_out = true;
+            break;
+          }
+          __nanosleep(32);
+        }
+      }
+    }
+    if (timed_out) atomicOr(&ctl->status, ST_TIMEOUT);
+    __syncwarp();
     for (int kp = r0; kp < di; kp++) {
       const int k = cols[kp];
-      if (lane == 0) wait_flag(flags, k, epoch, ctl);
-      __syncwarp();
-      // L_ik = A_ik * U_kk^{-1}
       const double* Ukk = LU + 36 * (size_t)diag[k];
       const double* Aik = LU + 36 * (size_t)kp;
       for (int t = lane; t < 36; t += 32) {
         const int r = t / 6, c = t % 6;
         double s = 0.0;
 #pragma unroll
-        for (int m = 0; m < 6; m++) s = fma(Aik[6 * r + m], __ldcg(&Ukk[6 * m + c]), s);
+        for (int m = 0; m < 6; m++) s = fma(__ldcg(&Aik[6 * r + m]), __ldcg(&Ukk[6 * m + c]), s);
         Lb[t] = s;
       }
       __syncwarp();
-      for (int t = lane; t < 36; t += 32) LU[36 * (size_t)kp + t] = Lb[t];
-      // A_ij -= L_ik U_kj for j > k in row k that are present in row i
+      for (int t = lane; t < 36; t += 32) __stcg(&LU[36 * (size_t)kp + t], Lb[t]);
       int tp = kp + 1;
       const int k1 = rowp[k + 1];
       for (int jp = diag[k] + 1; jp < k1; jp++) {
@@ -192,79 +247,28 @@ __global__ void __launch_bounds__(128) ilu_factor_kernel(
           double s = 0.0;
 #pragma unroll
           for (int m = 0; m < 6; m++) s = fma(Lb[6 * r + m], __ldcg(&Ukj[6 * m + c]), s);
-          Aij[t] -= s;
+          __stcg(&Aij[t], __ldcg(&Aij[t]) - s);
         }
       }
       __syncwarp();
     }
-    // invert the updated diagonal block in place
     double* Dii = LU + 36 * (size_t)di;
-    for (int t = lane; t < 36; t += 32) M[t] = Dii[t];
+    for (int t = lane; t < 36; t += 32) M[t] = __ldcg(&Dii[t]);
     __syncwarp();
-    inv6_warp(M, Inv, lane, ctl, i);
+    inv6_warp(M, Inv, lane, ctl, grow);
     for (int t = lane; t < 36; t += 32) {
       const double v = Inv[t];
       if (!isfinite(v)) {
         atomicOr(&ctl->status, ST_ZERO_PIVOT);
-        atomicCAS(&ctl->pivot, 0, i + 1);
+        atomicCAS(&ctl->pivot, 0, grow + 1);
       }
-      Dii[t] = v;
+      __stcg(&Dii[t], v);
     }
-    publish(flags, i, epoch, lane);
+    __syncwarp();
+    if (lane == 0) st_release(&flags[grow], epoch);
   }
 }
 
-// --------------------------------------------------------- triangular solves
-// Lower: y_i = r_i - sum_{k<i} L_ik y_k (unit block diagonal).
-// Upper: x_i = Uinv_ii (y_i - sum_{j>i} U_ij x_j).
-template <class VT, bool UPPER>
-__global__ void __launch_bounds__(128) trisolve_kernel(
-    int n, const int32_t* __restrict__ rowp, const int32_t* __restrict__ cols,
-    const int32_t* __restrict__ diag, const int32_t* __restrict__ order,
-    const VT* __restrict__ LU, const double* __restrict__ rhs, double* out, int* flags,
-    SweepCtl* ctl) {
-  const int lane = threadIdx.x & 31;
-  const int g = lane / 6, r = lane % 6;
-  const int epoch = ctl->epoch;
-  while (true) {
-    const int idx = fetch_row(ctl, lane);
-    if (idx >= n) break;
-    const int i = order[idx];
-    const int di = diag[i];
-    const int b0 = UPPER ? di + 1 : rowp[i];
-    const int b1 = UPPER ? rowp[i + 1] : di;
-    double acc = 0.0;
-    if (g < 4) {
-      for (int blk = b0 + g; blk < b1; blk += 4) {
-        const int k = cols[blk];
-        VT a[6];
-#pragma unroll
-        for (int c = 0; c < 6; c++) a[c] = LU[36 * (size_t)blk + 6 * r + c];
-        wait_flag(flags, k, epoch, ctl);
-        const double* xk = out + 6 * (size_t)k;
-#pragma unroll
-        for (int c = 0; c < 6; c++) acc = fma((double)a[c], __ldcg(&xk[c]), acc);
-      }
-    }
-    acc += __shfl_down_sync(0xffffffffu, acc, 12);
-    acc += __shfl_down_sync(0xffffffffu, acc, 6);
-    const double t = (lane < 6 ? rhs[6 * (size_t)i + lane] : 0.0) - acc;
-    if (!UPPER) {
-      if (lane < 6) __stcg(&out[6 * (size_t)i + lane], t);
-    } else {
-      double v = 0.0;
-#pragma unroll
-      for (int c = 0; c < 6; c++) {
-        const double tc = __shfl_sync(0xffffffffu, t, c);
-        if (lane < 6) v = fma((double)LU[36 * (size_t)di + 6 * lane + c], tc, v);
-      }
-      if (lane < 6) __stcg(&out[6 * (size_t)i + lane], v);
-    }
-    publish(flags, i, epoch, lane);
-  }
-}
-
-// ------------------------------------------------------------ small kernels
 __global__ void scatter_values_kernel(int nA, const int32_t* __restrict__ map,
                                       const double* __restrict__ A, double* __restrict__ LU) {
   const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -277,26 +281,858 @@ __global__ void convert_kernel(size_t n, const double* __restrict__ in, T2* __re
   if (t < n) out[t] = (T2)in[t];
 }
 
+// --------------------------------------------------------- triangular sweeps
+// Lower: y_i = r_i - sum_{k<i} L_ik y_k. Upper: x_i = Uinv_ii (y_i - sum_{j>i} U_ij x_j).
+// `out` must hold the sentinel for every row of a live problem on entry.
+template <class VT, bool UPPER>
+__global__ void __launch_bounds__(128) bsweep_kernel(int nrows, const int32_t* __restrict__ row_prob,
+                                                     const ProbDev* __restrict__ P,
+                                                     const int* __restrict__ live,
+                                                     const int32_t* __restrict__ order,
+                                                     const double* __restrict__ rhs, double* out,
+                                                     SweepCtl* ctl) {
+  const int lane = threadIdx.x & 31;
+  const int g = lane / 6, r = lane % 6;
+  int next = 0;
+  if (lane == 0) next = atomicAdd(&ctl->counter, 1);
+  next = __shfl_sync(0xffffffffu, next, 0);
+  bool timed_out = false;
+  while (next < nrows) {
+    const int idx = next;
+    if (lane == 0) next = atomicAdd(&ctl->counter, 1);  // prefetch the next row index
+    next = __shfl_sync(0xffffffffu, next, 0);
+    const int grow = order[idx];
+    const int p = row_prob[grow];
+    if (live && !live[p]) continue;
+    const ProbDev& d = P[p];
+    const int i = grow - d.off;
+    const VT* LU = sizeof(VT) == 8 ? (const VT*)d.LU64 : (const VT*)d.LU32;
+    const int di = d.pdiag[i];
+    const int b0 = UPPER ? di + 1 : d.prowp[i];
+    const int b1 = UPPER ? d.prowp[i + 1] : di;
+    double* ob = out + 6 * (size_t)d.off;
+    double acc = 0.0;
+    if (g < 4) {
+      for (int blk = b0 + g; blk < b1; blk += 4) {
+        const int k = d.pcols[blk];
+        VT a[6];
+#pragma unroll
+        for (int c = 0; c < 6; c++) a[c] = LU[36 * (size_t)blk + 6 * r + c];
+        const double* xk = ob + 6 * (size_t)k;
+        double xv[6];
+        const unsigned long long t0 = global_ns();
+        unsigned polls = 0;
+        while (true) {
+          bool ready = true;
+#pragma unroll
+          for (int c = 0; c < 6; c++) {
+            xv[c] = ld_relaxed(&xk[c]);
+            ready = ready && !is_sentinel(xv[c]);
+          }
+          if (ready) break;
+          if (wait_expired(t0, polls)) {
+            timed_out = true;
+            break;
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < 6; c++) acc = fma((double)a[c], xv[c], acc);
+      }
+    }
+    acc += __shfl_down_sync(0xffffffffu, acc, 12);
+    acc += __shfl_down_sync(0xffffffffu, acc, 6);
+    const double t = (lane < 6 ? rhs[6 * (size_t)grow + lane] : 0.0) - acc;
+    if (!UPPER) {
+      if (lane < 6) st_relaxed(&ob[6 * (size_t)i + lane], t);
+    } else {
+      double v = 0.0;
+#pragma unroll
+      for (int c = 0; c < 6; c++) {
+        const double tc = __shfl_sync(0xffffffffu, t, c);
+        if (lane < 6) v = fma((double)LU[36 * (size_t)di + 6 * lane + c], tc, v);
+      }
+      if (lane < 6) st_relaxed(&ob[6 * (size_t)i + lane], v);
+    }
+  }
+  if (timed_out) atomicOr(&ctl->status, ST_TIMEOUT);
+}
+
+// ------------------------------------------------- segmented vector kernels
+struct Chunks {
+  int n;                   // number of chunks
+  const int32_t* prob;     // chunk -> problem
+  const int64_t* lo;       // chunk start (doubles, batch space)
+  const int64_t* hi;       // chunk end
+  const int32_t* pstart;   // problem -> first chunk, [np + 1]
+};
+
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x == 0)
+    for (int k = 0; k < (int)(blockDim.x >> 5); k++) s += sh[k];
+  __syncthreads();
+  return s;
+}
+
+// partial[i * C.n + c] = V_i . w over chunk c, i = 0..jj, for running problems
+__global__ void seg_dots(const double* __restrict__ V, const double* __restrict__ w, size_t N,
+                         int jj, Chunks C, const int* __restrict__ run, double* partial) {
+  __shared__ double sh[32];
+  const int c = blockIdx.x;
+  if (!run[C.prob[c]]) return;
+  const int64_t lo = C.lo[c], hi = C.hi[c];
+  for (int i = 0; i <= jj; i++) {
+    const double* v = V + (size_t)i * N;
+    double acc = 0.0;
+    for (int64_t t = lo + threadIdx.x; t < hi; t += blockDim.x) acc = fma(v[t], w[t], acc);
+    const double s = block_sum(acc, sh);
+    if (threadIdx.x == 0) partial[(size_t)i * C.n + c] = s;
+  }
+}
+
+struct GmArrays {
+  double* H;       // np * (m+1) * m
+  double* g;       // np * (m+1)
+  double* cs;      // np * m
+  double* ss;      // np * m
+  double* y;       // np * m
+  double* h;       // np * (m+1)
+  double* hn;      // np
+  double* target;  // np
+  int* jcnt;       // np
+  int* run;        // np
+  int* live;       // np
+};
+
+// h_p[i] = sum over p's chunks; H_p[i][jj] (+)= h_p[i]
+__global__ void seg_reduce_dots(const double* partial, Chunks C, int jj, int m, GmArrays G,
+                                int acc) {
+  const int p = blockIdx.x;
+  if (!G.run[p]) return;
+  for (int i = threadIdx.x; i <= jj; i += blockDim.x) {
+    double s = 0.0;
+    for (int c = C.pstart[p]; c < C.pstart[p + 1]; c++) s += partial[(size_t)i * C.n + c];
+    G.h[(size_t)p * (m + 1) + i] = s;
+    double* Hij = &G.H[(size_t)p * (m + 1) * m + (size_t)i * m + jj];
+    *Hij = acc ? *Hij + s : s;
+  }
+}
+// w -= sum_{i<=jj} h_p[i] V_i over chunk c; optional per-chunk |w|^2
+__global__ void seg_update(const double* __restrict__ V, double* __restrict__ w, size_t N,
+                           int jj, int m, Chunks C, GmArrays G, double* pnorm) {
+  __shared__ double sh[32];
+  __shared__ double hs[1024];
+  const int c = blockIdx.x;
+  const int p = C.prob[c];
+  if (!G.run[p]) return;
+  for (int i = threadIdx.x; i <= jj; i += blockDim.x) hs[i] = G.h[(size_t)p * (m + 1) + i];
+  __syncthreads();
+  const int64_t lo = C.lo[c], hi = C.hi[c];
+  double acc = 0.0;
+  for (int64_t t = lo + threadIdx.x; t < hi; t += blockDim.x) {
+    double s = w[t];
+    for (int i = 0; i <= jj; i++) s = fma(-hs[i], V[(size_t)i * N + t], s);
+    w[t] = s;
+    acc = fma(s, s, acc);
+  }
+  if (pnorm) {
+    const double b = block_sum(acc, sh);
+    if (threadIdx.x == 0) pnorm[c] = b;
+  }
+}
+// per-chunk sum of squares over problems with mask[p] (all when mask is null)
+__global__ void seg_sumsq(const double* __restrict__ v, Chunks C, const int* __restrict__ mask,
+                          double* pnorm) {
+  __shared__ double sh[32];
+  const int c = blockIdx.x;
+  if (mask && !mask[C.prob[c]]) return;
+  double acc = 0.0;
+  for (int64_t t = C.lo[c] + threadIdx.x; t < C.hi[c]; t += blockDim.x)
+    acc = fma(v[t], v[t], acc);
+  const double b = block_sum(acc, sh);
+  if (threadIdx.x == 0) pnorm[c] = b;
+}
+__global__ void seg_norm_out(const double* pnorm, Chunks C, int np, const int* mask,
+                             double* out) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= np) return;
+  if (mask && !mask[p]) return;
+  double s = 0.0;
+  for (int c = C.pstart[p]; c < C.pstart[p + 1]; c++) s += pnorm[c];
+  out[p] = sqrt(s);
+}
+__global__ void seg_norm_finish(const double* pnorm, Chunks C, int np, int jj, int m,
+                                GmArrays G) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= np || !G.run[p]) return;
+  double s = 0.0;
+  for (int c = C.pstart[p]; c < C.pstart[p + 1]; c++) s += pnorm[c];
+  G.hn[p] = sqrt(s);
+  G.H[(size_t)p * (m + 1) * m + (size_t)(jj + 1) * m + jj] = G.hn[p];
+}
+__global__ void seg_scale(const double* __restrict__ src, double* __restrict__ dst, Chunks C,
+                          const int* __restrict__ run, const double* __restrict__ hn) {
+  const int c = blockIdx.x;
+  const int p = C.prob[c];
+  if (!run[p]) return;
+  const double inv = hn[p] > 0.0 ? 1.0 / hn[p] : 0.0;
+  for (int64_t t = C.lo[c] + threadIdx.x; t < C.hi[c]; t += blockDim.x) dst[t] = src[t] * inv;
+}
+// Givens update of column jj (examples/iterative/gmres.cu:672-699) per problem
+__global__ void bgivens(int np, int jj, int m, int step_limit, GmArrays G) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= np || !G.run[p]) return;
+  double* H = G.H + (size_t)p * (m + 1) * m;
+  double* g = G.g + (size_t)p * (m + 1);
+  double* cs = G.cs + (size_t)p * m;
+  double* ss = G.ss + (size_t)p * m;
+  for (int i = 0; i < jj; i++) {
+    const double a = H[(size_t)i * m + jj], c = H[(size_t)(i + 1) * m + jj];
+    H[(size_t)i * m + jj] = cs[i] * a + ss[i] * c;
+    H[(size_t)(i + 1) * m + jj] = -ss[i] * a + cs[i] * c;
+  }
+  const double a = H[(size_t)jj * m + jj], c = H[(size_t)(jj + 1) * m + jj];
+  const double hyp = sqrt(a * a + c * c);
+  cs[jj] = hyp > 0.0 ? a / hyp : 1.0;
+  ss[jj] = hyp > 0.0 ? c / hyp : 0.0;
+  H[(size_t)jj * m + jj] = cs[jj] * a + ss[jj] * c;
+  H[(size_t)(jj + 1) * m + jj] = 0.0;
+  g[jj + 1] = -ss[jj] * g[jj];
+  g[jj] = cs[jj] * g[jj];
+  G.jcnt[p] = jj + 1;
+  if (fabs(g[jj + 1]) <= G.target[p] || G.hn[p] == 0.0 || !isfinite(g[jj + 1]) ||
+      jj + 1 >= step_limit)
+    G.run[p] = 0;
+}
+__global__ void bbacksolve(int np, int m, GmArrays G) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= np || !G.live[p]) return;
+  const int j = G.jcnt[p];
+  const double* H = G.H + (size_t)p * (m + 1) * m;
+  const double* g = G.g + (size_t)p * (m + 1);
+  double* y = G.y + (size_t)p * m;
+  for (int i = j - 1; i >= 0; i--) {
+    double s = g[i];
+    for (int k = i + 1; k < j; k++) s -= H[(size_t)i * m + k] * y[k];
+    y[i] = s / H[(size_t)i * m + i];
+  }
+}
+// out = sum_{i < jcnt_p} y_p[i] V_i over live problems (zero otherwise)
+__global__ void seg_combine(const double* __restrict__ V, size_t N, int m, Chunks C, GmArrays G,
+                            double* __restrict__ out) {
+  __shared__ double ys[1024];
+  const int c = blockIdx.x;
+  const int p = C.prob[c];
+  const int j = G.live[p] ? G.jcnt[p] : 0;
+  for (int i = threadIdx.x; i < j; i += blockDim.x) ys[i] = G.y[(size_t)p * m + i];
+  __syncthreads();
+  for (int64_t t = C.lo[c] + threadIdx.x; t < C.hi[c]; t += blockDim.x) {
+    double s = 0.0;
+    for (int i = 0; i < j; i++) s = fma(ys[i], V[(size_t)i * N + t], s);
+    out[t] = s;
+  }
+}
+// cycle start: beta_p = ||src_p||, g_p = (beta, 0, ...), run_p = live_p
+__global__ void bcycle_init(const double* pnorm, Chunks C, int np, int m, GmArrays G) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= np) return;
+  double s = 0.0;
+  if (G.live[p])
+    for (int c = C.pstart[p]; c < C.pstart[p + 1]; c++) s += pnorm[c];
+  const double beta = sqrt(s);
+  G.hn[p] = beta;
+  G.jcnt[p] = 0;
+  G.run[p] = (G.live[p] && beta > 0.0) ? 1 : 0;
+  double* g = G.g + (size_t)p * (m + 1);
+  g[0] = beta;
+  for (int i = 1; i <= m; i++) g[i] = 0.0;
+}
+// y += a * x over problems with mask[p] (all when mask is null)
+__global__ void seg_axpy(double a, const double* __restrict__ x, double* __restrict__ y,
+                         Chunks C, const int* __restrict__ mask) {
+  const int c = blockIdx.x;
+  if (mask && !mask[C.prob[c]]) return;
+  for (int64_t t = C.lo[c] + threadIdx.x; t < C.hi[c]; t += blockDim.x) y[t] += a * x[t];
+}
+__global__ void seg_copy(const double* __restrict__ x, double* __restrict__ y, Chunks C,
+                         const int* __restrict__ mask) {
+  const int c = blockIdx.x;
+  if (mask && !mask[C.prob[c]]) return;
+  for (int64_t t = C.lo[c] + threadIdx.x; t < C.hi[c]; t += blockDim.x) y[t] = x[t];
+}
+__global__ void set_target(int np, const double* norms, double rtol, GmArrays G) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < np) G.target[p] = rtol * norms[p];
+}
+// natural <-> batch-space permutation, one problem per blockIdx.y
+struct PermEntry {
+  const int32_t* perm;
+  int n, off;
+  const double* in;
+  double* out;
+};
+__global__ void bpermute(const PermEntry* E, int dir) {
+  const PermEntry e = E[blockIdx.y];
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 6 * e.n; t += gridDim.x * blockDim.x) {
+    const int i = t / 6, k = t % 6;
+    if (dir == 0)
+      e.out[6 * ((size_t)e.off + e.perm[i]) + k] = e.in[t];
+    else
+      e.out[t] = e.in[6 * ((size_t)e.off + e.perm[i]) + k];
+  }
+}
+
 }  // namespace gf
 
 using namespace gf;
 
+// ---------------------------------------------------------------- handles
 struct gf_precond {
   gf_assembler* a = nullptr;
   int fill = 0, prec = GF_PREC_FP64;
   Pattern pat;
   int nlevL = 0, nlevU = 0;
-  DevBuf<int32_t> d_rowp, d_cols, d_diag, d_orderL, d_orderU, d_amap, d_flags;
+  std::vector<int32_t> lvL, lvU;
+  DevBuf<int32_t> d_rowp, d_cols, d_diag, d_amap;
   DevBuf<double> d_lu;
   DevBuf<float> d_lu32;
-  DevBuf<double> d_tmp;
+  gf_batch* self = nullptr;  // batch of one, built on first use
+};
+
+struct gf_batch {
+  int np = 0, nrows = 0, maxlevL = 0, maxlevU = 0;
+  size_t N = 0;  // doubles in batch space
+  std::vector<gf_assembler*> asms;
+  std::vector<gf_bsr*> mats;
+  std::vector<gf_precond*> pcs;
+  std::vector<int> offs;
+  DevBuf<ProbDev> d_desc;
+  DevBuf<int32_t> d_row_prob, d_orderL, d_orderU, d_flags;
   DevBuf<SweepCtl> d_ctl;
+  DevBuf<double> d_tmp, d_b, d_x;
+  int nchunks = 0;
+  DevBuf<int32_t> d_cprob, d_pstart;
+  DevBuf<int64_t> d_clo, d_chi;
+  DevBuf<PermEntry> d_perm_b, d_perm_x, d_perm_out;
+  int m = 0;
+  DevBuf<double> V, H, g, cs, ss, y, h, hn, target, partial, pnorm, w, t, r, d, e, norms, bnorm;
+  DevBuf<int> jcnt, run, live, live2;
+  Chunks chunks() const { return Chunks{nchunks, d_cprob.p, d_clo.p, d_chi.p, d_pstart.p}; }
 };
 
 namespace gf {
-gf_status precond_apply_impl(gf_precond* p, const double* r, double* z, cudaStream_t st);
+
+static int sm_count() {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms;
 }
 
+// Descriptor table (rebuilt when a buffer such as the FP32 matrix copy is
+// allocated).
+static gf_status upload_desc(gf_batch* B) {
+  std::vector<ProbDev> h(B->np);
+  for (int k = 0; k < B->np; k++) {
+    gf_assembler* a = B->asms[k];
+    gf_precond* p = B->pcs[k];
+    ProbDev& d = h[k];
+    d.n = a->nnodes;
+    d.off = B->offs[k];
+    d.rowp = a->d_rowp.p;
+    d.cols = a->d_cols.p;
+    d.A64 = B->mats[k]->vals.p;
+    d.A32 = B->mats[k]->vals32.p;
+    d.prowp = p->d_rowp.p;
+    d.pcols = p->d_cols.p;
+    d.pdiag = p->d_diag.p;
+    d.LU64 = p->d_lu.p;
+    d.LU32 = p->d_lu32.p;
+  }
+  GF_CUDA(cudaMemcpy(B->d_desc.p, h.data(), sizeof(ProbDev) * B->np, cudaMemcpyHostToDevice));
+  return GF_OK;
+}
+
+static gf_status batch_build(gf_batch* B) {
+  const int np = B->np;
+  B->offs.resize(np + 1);
+  B->offs[0] = 0;
+  for (int k = 0; k < np; k++) B->offs[k + 1] = B->offs[k] + B->asms[k]->nnodes;
+  B->nrows = B->offs[np];
+  B->N = (size_t)6 * B->nrows;
+  std::vector<int32_t> row_prob(B->nrows);
+  // merged level orders: (level, problem, row)
+  std::vector<std::array<int, 3>> keysL, keysU;
+  keysL.reserve(B->nrows);
+  keysU.reserve(B->nrows);
+  B->maxlevL = B->maxlevU = 0;
+  for (int k = 0; k < np; k++) {
+    gf_precond* p = B->pcs[k];
+    for (int i = 0; i < B->asms[k]->nnodes; i++) {
+      row_prob[B->offs[k] + i] = k;
+      keysL.push_back({p->lvL[i], k, i});
+      keysU.push_back({p->lvU[i], k, i});
+    }
+    B->maxlevL = std::max(B->maxlevL, p->nlevL);
+    B->maxlevU = std::max(B->maxlevU, p->nlevU);
+  }
+  std::sort(keysL.begin(), keysL.end());
+  std::sort(keysU.begin(), keysU.end());
+  std::vector<int32_t> ordL(B->nrows), ordU(B->nrows);
+  for (int t = 0; t < B->nrows; t++) {
+    ordL[t] = B->offs[keysL[t][1]] + keysL[t][2];
+    ordU[t] = B->offs[keysU[t][1]] + keysU[t][2];
+  }
+  // reduction chunks aligned to each problem
+  std::vector<int32_t> cprob, pstart(np + 1);
+  std::vector<int64_t> clo, chi;
+  for (int k = 0; k < np; k++) {
+    pstart[k] = (int32_t)cprob.size();
+    const int64_t lo = 6ll * B->offs[k], hi = 6ll * B->offs[k + 1];
+    for (int64_t s = lo; s < hi; s += kChunk) {
+      cprob.push_back(k);
+      clo.push_back(s);
+      chi.push_back(std::min(hi, s + (int64_t)kChunk));
+    }
+  }
+  pstart[np] = (int32_t)cprob.size();
+  B->nchunks = (int)cprob.size();
+  cudaError_t e = cudaSuccess;
+  auto up = [&](cudaError_t x) {
+    if (e == cudaSuccess) e = x;
+  };
+  up(B->d_desc.alloc(np));
+  up(B->d_row_prob.upload(row_prob));
+  up(B->d_orderL.upload(ordL));
+  up(B->d_orderU.upload(ordU));
+  up(B->d_flags.alloc(B->nrows));
+  if (e == cudaSuccess) up(cudaMemset(B->d_flags.p, 0, sizeof(int32_t) * B->nrows));
+  up(B->d_ctl.alloc(1));
+  if (e == cudaSuccess) up(cudaMemset(B->d_ctl.p, 0, sizeof(SweepCtl)));
+  up(B->d_tmp.alloc(B->N));
+  up(B->d_b.alloc(B->N));
+  up(B->d_x.alloc(B->N));
+  up(B->d_cprob.upload(cprob));
+  up(B->d_pstart.upload(pstart));
+  up(B->d_clo.upload(clo));
+  up(B->d_chi.upload(chi));
+  up(B->d_perm_b.alloc(np));
+  up(B->d_perm_x.alloc(np));
+  up(B->d_perm_out.alloc(np));
+  up(B->norms.alloc(np));
+  up(B->bnorm.alloc(np));
+  up(B->live2.alloc(np));
+  if (e != cudaSuccess) {
+    set_last_error("batch build", e);
+    return e == cudaErrorMemoryAllocation ? GF_OOM : GF_CUDA_ERROR;
+  }
+  return upload_desc(B);
+}
+
+static gf_status ensure_gmres(gf_batch* B, int m) {
+  if (B->m == m) return GF_OK;
+  const int np = B->np;
+  cudaError_t e = cudaSuccess;
+  auto al = [&](cudaError_t x) {
+    if (e == cudaSuccess) e = x;
+  };
+  al(B->V.alloc((size_t)(m + 1) * B->N));
+  al(B->H.alloc((size_t)np * (m + 1) * m));
+  al(B->g.alloc((size_t)np * (m + 1)));
+  al(B->cs.alloc((size_t)np * m));
+  al(B->ss.alloc((size_t)np * m));
+  al(B->y.alloc((size_t)np * m));
+  al(B->h.alloc((size_t)np * (m + 1)));
+  al(B->hn.alloc(np));
+  al(B->target.alloc(np));
+  al(B->partial.alloc((size_t)(m + 1) * B->nchunks));
+  al(B->pnorm.alloc(B->nchunks));
+  al(B->w.alloc(B->N));
+  al(B->t.alloc(B->N));
+  al(B->r.alloc(B->N));
+  al(B->d.alloc(B->N));
+  al(B->e.alloc(B->N));
+  al(B->jcnt.alloc(np));
+  al(B->run.alloc(np));
+  al(B->live.alloc(np));
+  if (e != cudaSuccess) {
+    set_last_error("gmres workspace", e);
+    B->m = 0;
+    return e == cudaErrorMemoryAllocation ? GF_OOM : GF_CUDA_ERROR;
+  }
+  GF_CUDA(cudaMemset(B->H.p, 0, sizeof(double) * B->H.n));
+  B->m = m;
+  return GF_OK;
+}
+
+static GmArrays arrays(gf_batch* B) {
+  return GmArrays{B->H.p,  B->g.p,      B->cs.p,   B->ss.p,  B->y.p,   B->h.p,
+                  B->hn.p, B->target.p, B->jcnt.p, B->run.p, B->live.p};
+}
+
+static unsigned persistent_grid(int nrows) {
+  return (unsigned)std::max(1, std::min(sm_count() * 4, (nrows + 3) / 4));
+}
+
+// z = U^{-1} L^{-1} r for problems with live[p] (all when live is null)
+template <class VT>
+static gf_status bprecond(gf_batch* B, const int* live, const double* r, double* z,
+                          cudaStream_t st) {
+  const unsigned nb = persistent_grid(B->nrows);
+  fill_sentinel<<<592, 256, 0, st>>>(B->d_tmp.p, B->N); ::gf::count_launch();
+  fill_sentinel<<<592, 256, 0, st>>>(z, B->N); ::gf::count_launch();
+  sweep_begin<<<1, 1, 0, st>>>(B->d_ctl.p); ::gf::count_launch();
+  bsweep_kernel<VT, false><<<nb, 128, 0, st>>>(B->nrows, B->d_row_prob.p, B->d_desc.p, live,
+                                               B->d_orderL.p, r, B->d_tmp.p, B->d_ctl.p); ::gf::count_launch();
+  sweep_begin<<<1, 1, 0, st>>>(B->d_ctl.p); ::gf::count_launch();
+  bsweep_kernel<VT, true><<<nb, 128, 0, st>>>(B->nrows, B->d_row_prob.p, B->d_desc.p, live,
+                                              B->d_orderU.p, B->d_tmp.p, z, B->d_ctl.p); ::gf::count_launch();
+  GF_CHECK_LAUNCH();
+  return GF_OK;
+}
+
+template <class VT>
+static gf_status bspmv(gf_batch* B, const int* live, const double* x, double alpha, double beta,
+                       double* y, cudaStream_t st) {
+  bspmv_kernel<VT><<<(B->nrows + 7) / 8, 256, 0, st>>>(B->nrows, B->d_row_prob.p, B->d_desc.p,
+                                                       live, x, alpha, beta, y); ::gf::count_launch();
+  GF_CHECK_LAUNCH();
+  return GF_OK;
+}
+
+static gf_status read_ctl(gf_batch* B, cudaStream_t st, SweepCtl* h) {
+  GF_CUDA(cudaMemcpyAsync(h, B->d_ctl.p, sizeof(SweepCtl), cudaMemcpyDeviceToHost, st));
+  GF_CUDA(cudaStreamSynchronize(st));
+  return GF_OK;
+}
+
+static gf_status batch_factor(gf_batch* B, cudaStream_t st) {
+  for (int k = 0; k < B->np; k++) {
+    gf_precond* p = B->pcs[k];
+    const size_t nv = (size_t)36 * p->pat.nnz();
+    GF_CUDA(cudaMemsetAsync(p->d_lu.p, 0, sizeof(double) * nv, st));
+    const size_t na = (size_t)36 * p->a->pat.nnz();
+    scatter_values_kernel<<<(unsigned)((na + 255) / 256), 256, 0, st>>>(
+        p->a->pat.nnz(), p->d_amap.p, B->mats[k]->vals.p, p->d_lu.p); ::gf::count_launch();
+  }
+  GF_CHECK_LAUNCH();
+  GF_CUDA(cudaMemsetAsync(&B->d_ctl.p->status, 0, 2 * sizeof(int), st));
+  sweep_begin<<<1, 1, 0, st>>>(B->d_ctl.p); ::gf::count_launch();
+  bfactor_kernel<<<persistent_grid(B->nrows), 128, 0, st>>>(B->nrows, B->d_row_prob.p,
+                                                            B->d_desc.p, B->d_orderL.p,
+                                                            B->d_flags.p, B->d_ctl.p); ::gf::count_launch();
+  GF_CHECK_LAUNCH();
+  for (int k = 0; k < B->np; k++) {
+    gf_precond* p = B->pcs[k];
+    if (p->prec == GF_PREC_FP32) {
+      const size_t nv = (size_t)36 * p->pat.nnz();
+      convert_kernel<float><<<(unsigned)((nv + 255) / 256), 256, 0, st>>>(nv, p->d_lu.p,
+                                                                          p->d_lu32.p); ::gf::count_launch();
+    }
+  }
+  GF_CHECK_LAUNCH();
+  SweepCtl h;
+  gf_status s = read_ctl(B, st, &h);
+  if (s != GF_OK) return s;
+  if (h.status & ST_TIMEOUT) return GF_TIMEOUT;
+  if (h.status & ST_ZERO_PIVOT) return GF_ZERO_PIVOT;
+  return GF_OK;
+}
+
+// Batched restarted GMRES on A x = b (batch space) for problems with
+// live0[p] != 0. side 1: right preconditioning (Givens residual = true
+// residual); side 0: left (the reference's choice). Per-problem outputs:
+// iters, restarts, rel (true ||b - A x|| / ||b||).
+template <class VT>
+static gf_status bgmres(gf_batch* B, const double* b, double* x, int m, int max_it, double rtol,
+                        int side, int check_every, const std::vector<int>& live0,
+                        std::vector<int>& iters, std::vector<int>& restarts,
+                        std::vector<double>& rel, cudaStream_t st) {
+  const int np = B->np;
+  gf_status s = ensure_gmres(B, m);
+  if (s != GF_OK) return s;
+  const Chunks C = B->chunks();
+  const GmArrays G = arrays(B);
+  const int nc = B->nchunks;
+  const int pb = (np + 127) / 128;
+  std::vector<double> bn(np, 1.0), rn(np);
+  GF_CUDA(cudaMemcpyAsync(B->live.p, live0.data(), sizeof(int) * np, cudaMemcpyHostToDevice, st));
+  seg_sumsq<<<nc, kRedThreads, 0, st>>>(b, C, nullptr, B->pnorm.p); ::gf::count_launch();
+  seg_norm_out<<<pb, 128, 0, st>>>(B->pnorm.p, C, np, nullptr, B->bnorm.p); ::gf::count_launch();
+  GF_CUDA(cudaMemcpyAsync(bn.data(), B->bnorm.p, sizeof(double) * np, cudaMemcpyDeviceToHost, st));
+  if (side == 0) {
+    s = bprecond<VT>(B, B->live.p, b, B->t.p, st);
+    if (s != GF_OK) return s;
+    seg_sumsq<<<nc, kRedThreads, 0, st>>>(B->t.p, C, B->live.p, B->pnorm.p); ::gf::count_launch();
+    seg_norm_out<<<pb, 128, 0, st>>>(B->pnorm.p, C, np, B->live.p, B->norms.p); ::gf::count_launch();
+    set_target<<<pb, 128, 0, st>>>(np, B->norms.p, rtol, G); ::gf::count_launch();
+  } else {
+    set_target<<<pb, 128, 0, st>>>(np, B->bnorm.p, rtol, G); ::gf::count_launch();
+  }
+  GF_CHECK_LAUNCH();
+  GF_CUDA(cudaStreamSynchronize(st));
+  for (int p = 0; p < np; p++)
+    if (bn[p] == 0.0) bn[p] = 1.0;
+  std::vector<int> live = live0, jc(np), runh(np);
+  iters.assign(np, 0);
+  restarts.assign(np, 0);
+  rel.assign(np, 0.0);
+  int steps_total = 0;
+  bool first = true;
+  while (true) {
+    // r = b - A x and the true relative residual of every live problem
+    seg_copy<<<nc, kRedThreads, 0, st>>>(b, B->r.p, C, B->live.p); ::gf::count_launch();
+    s = bspmv<VT>(B, B->live.p, x, -1.0, 1.0, B->r.p, st);
+    if (s != GF_OK) return s;
+    seg_sumsq<<<nc, kRedThreads, 0, st>>>(B->r.p, C, B->live.p, B->pnorm.p); ::gf::count_launch();
+    seg_norm_out<<<pb, 128, 0, st>>>(B->pnorm.p, C, np, B->live.p, B->norms.p); ::gf::count_launch();
+    GF_CUDA(cudaMemcpyAsync(rn.data(), B->norms.p, sizeof(double) * np, cudaMemcpyDeviceToHost,
+                            st));
+    GF_CUDA(cudaStreamSynchronize(st));
+    bool any = false, bad = false;
+    for (int p = 0; p < np; p++) {
+      if (!live[p]) continue;
+      rel[p] = rn[p] / bn[p];
+      if (!std::isfinite(rel[p])) {
+        bad = true;
+        live[p] = 0;
+      } else if (rel[p] <= rtol) {
+        live[p] = 0;
+      } else {
+        any = true;
+        if (!first) restarts[p]++;
+      }
+    }
+    first = false;
+    if (bad) return GF_NAN;
+    if (!any || steps_total >= max_it) break;
+    GF_CUDA(cudaMemcpyAsync(B->live.p, live.data(), sizeof(int) * np, cudaMemcpyHostToDevice,
+                            st));
+    const double* src = B->r.p;
+    if (side == 0) {
+      s = bprecond<VT>(B, B->live.p, B->r.p, B->t.p, st);
+      if (s != GF_OK) return s;
+      src = B->t.p;
+    }
+    seg_sumsq<<<nc, kRedThreads, 0, st>>>(src, C, B->live.p, B->pnorm.p); ::gf::count_launch();
+    bcycle_init<<<pb, 128, 0, st>>>(B->pnorm.p, C, np, m, G); ::gf::count_launch();
+    seg_scale<<<nc, kRedThreads, 0, st>>>(src, B->V.p, C, B->run.p, B->hn.p); ::gf::count_launch();
+    GF_CHECK_LAUNCH();
+    const int steps = std::min(m, max_it - steps_total);
+    int jj = 0;
+    while (jj < steps) {
+      const int batch = std::min(check_every, steps - jj);
+      for (int k = 0; k < batch; k++, jj++) {
+        const double* vj = B->V.p + (size_t)jj * B->N;
+        if (side == 0) {
+          s = bspmv<VT>(B, B->run.p, vj, 1.0, 0.0, B->t.p, st);
+          if (s == GF_OK) s = bprecond<VT>(B, B->run.p, B->t.p, B->w.p, st);
+        } else {
+          s = bprecond<VT>(B, B->run.p, vj, B->t.p, st);
+          if (s == GF_OK) s = bspmv<VT>(B, B->run.p, B->t.p, 1.0, 0.0, B->w.p, st);
+        }
+        if (s != GF_OK) return s;
+        seg_dots<<<nc, kRedThreads, 0, st>>>(B->V.p, B->w.p, B->N, jj, C, B->run.p,
+                                              B->partial.p); ::gf::count_launch();
+        seg_reduce_dots<<<np, 128, 0, st>>>(B->partial.p, C, jj, m, G, 0); ::gf::count_launch();
+        seg_update<<<nc, kRedThreads, 0, st>>>(B->V.p, B->w.p, B->N, jj, m, C, G, nullptr); ::gf::count_launch();
+        seg_dots<<<nc, kRedThreads, 0, st>>>(B->V.p, B->w.p, B->N, jj, C, B->run.p,
+                                              B->partial.p); ::gf::count_launch();
+        seg_reduce_dots<<<np, 128, 0, st>>>(B->partial.p, C, jj, m, G, 1); ::gf::count_launch();
+        seg_update<<<nc, kRedThreads, 0, st>>>(B->V.p, B->w.p, B->N, jj, m, C, G, B->pnorm.p); ::gf::count_launch();
+        seg_norm_finish<<<pb, 128, 0, st>>>(B->pnorm.p, C, np, jj, m, G); ::gf::count_launch();
+        seg_scale<<<nc, kRedThreads, 0, st>>>(B->w.p, B->V.p + (size_t)(jj + 1) * B->N, C,
+                                               B->run.p, B->hn.p); ::gf::count_launch();
+        bgivens<<<pb, 128, 0, st>>>(np, jj, m, steps, G); ::gf::count_launch();
+        GF_CHECK_LAUNCH();
+      }
+      GF_CUDA(cudaMemcpyAsync(runh.data(), B->run.p, sizeof(int) * np, cudaMemcpyDeviceToHost,
+                              st));
+      GF_CUDA(cudaStreamSynchronize(st));
+      if (std::all_of(runh.begin(), runh.end(), [](int v) { return v == 0; })) break;
+    }
+    SweepCtl hc;
+    s = read_ctl(B, st, &hc);
+    if (s != GF_OK) return s;
+    if (hc.status & ST_TIMEOUT) return GF_TIMEOUT;
+    bbacksolve<<<pb, 128, 0, st>>>(np, m, G); ::gf::count_launch();
+    seg_combine<<<nc, kRedThreads, 0, st>>>(B->V.p, B->N, m, C, G, B->w.p); ::gf::count_launch();
+    GF_CHECK_LAUNCH();
+    if (side == 1) {
+      s = bprecond<VT>(B, B->live.p, B->w.p, B->t.p, st);
+      if (s != GF_OK) return s;
+      seg_axpy<<<nc, kRedThreads, 0, st>>>(1.0, B->t.p, x, C, B->live.p); ::gf::count_launch();
+    } else {
+      seg_axpy<<<nc, kRedThreads, 0, st>>>(1.0, B->w.p, x, C, B->live.p); ::gf::count_launch();
+    }
+    GF_CHECK_LAUNCH();
+    GF_CUDA(cudaMemcpyAsync(jc.data(), B->jcnt.p, sizeof(int) * np, cudaMemcpyDeviceToHost, st));
+    GF_CUDA(cudaStreamSynchronize(st));
+    int mx = 0;
+    for (int p = 0; p < np; p++)
+      if (live[p]) {
+        iters[p] += jc[p];
+        mx = std::max(mx, jc[p]);
+      }
+    steps_total += mx;
+  }
+  return GF_OK;
+}
+
+// Full solve of the batch (vectors in batch space): FP64 GMRES, or FP64
+// iterative refinement around an FP32-valued inner GMRES (FP32 SpMV + FP32
+// ILU apply with FP64 vectors and accumulation).
+static gf_status batch_solve_space(gf_batch* B, const gf_solve_opts& o,
+                                   std::vector<gf_solve_stats>& S, cudaStream_t st) {
+  const int np = B->np;
+  auto t0 = std::chrono::steady_clock::now();
+  std::vector<int> live(np, 1), iters, rest;
+  std::vector<double> rel;
+  S.assign(np, gf_solve_stats{});
+  gf_status result = GF_OK;
+  if (!o.mixed) {
+    result = bgmres<double>(B, B->d_b.p, B->d_x.p, o.restart, o.max_iters, o.rtol, o.side,
+                            o.check_every, live, iters, rest, rel, st);
+    for (int p = 0; p < np && !iters.empty(); p++) {
+      S[p].iterations = iters[p];
+      S[p].restarts = rest[p];
+      S[p].rel_residual = rel[p];
+    }
+  } else {
+    for (int k = 0; k < np; k++) {
+      gf_bsr* A = B->mats[k];
+      const size_t n36 = (size_t)36 * A->a->pat.nnz();
+      if (A->vals32.n != n36) {
+        GF_CUDA(A->vals32.alloc(n36));
+        gf_status s2 = upload_desc(B);
+        if (s2 != GF_OK) return s2;
+      }
+      convert_kernel<float><<<(unsigned)((n36 + 255) / 256), 256, 0, st>>>(n36, A->vals.p,
+                                                                           A->vals32.p); ::gf::count_launch();
+    }
+    GF_CHECK_LAUNCH();
+    gf_status s = ensure_gmres(B, o.restart);
+    if (s != GF_OK) return s;
+    const Chunks C = B->chunks();
+    const int nc = B->nchunks, pb = (np + 127) / 128;
+    std::vector<double> bn(np), rn(np);
+    seg_sumsq<<<nc, kRedThreads, 0, st>>>(B->d_b.p, C, nullptr, B->pnorm.p); ::gf::count_launch();
+    seg_norm_out<<<pb, 128, 0, st>>>(B->pnorm.p, C, np, nullptr, B->bnorm.p); ::gf::count_launch();
+    GF_CUDA(cudaMemcpyAsync(bn.data(), B->bnorm.p, sizeof(double) * np, cudaMemcpyDeviceToHost,
+                            st));
+    GF_CUDA(cudaStreamSynchronize(st));
+    for (int p = 0; p < np; p++)
+      if (bn[p] == 0.0) bn[p] = 1.0;
+    std::vector<int> tot_it(np, 0), tot_rs(np, 0), nref(np, 0);
+    std::vector<double> relv(np, 1.0);
+    int refine = 0;
+    while (true) {
+      GF_CUDA(cudaMemcpyAsync(B->live2.p, live.data(), sizeof(int) * np, cudaMemcpyHostToDevice,
+                              st));
+      seg_copy<<<nc, kRedThreads, 0, st>>>(B->d_b.p, B->d.p, C, B->live2.p); ::gf::count_launch();
+      s = bspmv<double>(B, B->live2.p, B->d_x.p, -1.0, 1.0, B->d.p, st);
+      if (s != GF_OK) return s;
+      seg_sumsq<<<nc, kRedThreads, 0, st>>>(B->d.p, C, B->live2.p, B->pnorm.p); ::gf::count_launch();
+      seg_norm_out<<<pb, 128, 0, st>>>(B->pnorm.p, C, np, B->live2.p, B->norms.p); ::gf::count_launch();
+      GF_CUDA(cudaMemcpyAsync(rn.data(), B->norms.p, sizeof(double) * np,
+                              cudaMemcpyDeviceToHost, st));
+      GF_CUDA(cudaStreamSynchronize(st));
+      bool any = false;
+      for (int p = 0; p < np; p++) {
+        if (!live[p]) continue;
+        relv[p] = rn[p] / bn[p];
+        if (!std::isfinite(relv[p])) {
+          result = GF_NAN;
+          live[p] = 0;
+        } else if (relv[p] <= o.rtol) {
+          live[p] = 0;
+        } else {
+          any = true;
+        }
+      }
+      if (!any || refine >= o.max_refine) break;
+      int maxit = 0;
+      for (int p = 0; p < np; p++)
+        if (live[p]) maxit = std::max(maxit, o.max_iters - tot_it[p]);
+      if (maxit <= 0) break;
+      // inner solve A32 e = r from zero
+      GF_CUDA(cudaMemsetAsync(B->e.p, 0, sizeof(double) * B->N, st));
+      s = bgmres<float>(B, B->d.p, B->e.p, o.restart, maxit, o.inner_rtol, o.side,
+                        o.check_every, live, iters, rest, rel, st);
+      if (s != GF_OK) {
+        result = s;
+        break;
+      }
+      GF_CUDA(cudaMemcpyAsync(B->live2.p, live.data(), sizeof(int) * np, cudaMemcpyHostToDevice,
+                              st));
+      seg_axpy<<<nc, kRedThreads, 0, st>>>(1.0, B->e.p, B->d_x.p, C, B->live2.p); ::gf::count_launch();
+      GF_CHECK_LAUNCH();
+      for (int p = 0; p < np; p++)
+        if (live[p]) {
+          tot_it[p] += iters[p];
+          tot_rs[p] += rest[p];
+          nref[p]++;
+        }
+      refine++;
+    }
+    for (int p = 0; p < np; p++) {
+      S[p].iterations = tot_it[p];
+      S[p].restarts = tot_rs[p];
+      S[p].refinements = nref[p];
+      S[p].rel_residual = relv[p];
+    }
+  }
+  const double ms =
+      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  for (int p = 0; p < np; p++) {
+    S[p].time_ms = ms;
+    gf_status sp = result;
+    if (sp == GF_OK && !(S[p].rel_residual <= o.rtol)) sp = GF_NOT_CONVERGED;
+    S[p].status = sp;
+    if (result == GF_OK && sp != GF_OK) result = sp;
+  }
+  return result;
+}
+
+static gf_status batch_create_impl(int n, gf_assembler* const* asms, gf_bsr* const* mats,
+                                   gf_precond* const* pcs, gf_batch** out) {
+  gf_batch* B = new gf_batch();
+  B->np = n;
+  B->asms.assign(asms, asms + n);
+  B->mats.assign(mats, mats + n);
+  B->pcs.assign(pcs, pcs + n);
+  gf_status s = batch_build(B);
+  if (s != GF_OK) {
+    delete B;
+    return s;
+  }
+  *out = B;
+  return GF_OK;
+}
+
+static gf_status self_batch(gf_precond* p, gf_bsr* A) {
+  if (p->self && p->self->mats[0] == A) return GF_OK;
+  if (p->self) {
+    delete p->self;
+    p->self = nullptr;
+  }
+  gf_assembler* a = p->a;
+  return batch_create_impl(1, &a, &A, &p, &p->self);
+}
+
+static bool opts_ok(const gf_solve_opts& o) {
+  return o.restart >= 1 && o.restart <= 1000 && o.max_iters >= 1 && o.rtol > 0.0 &&
+         o.check_every >= 1 && (o.side == 0 || o.side == 1) && o.max_refine >= 0 &&
+         (!o.mixed || o.inner_rtol > 0.0);
+}
+
+}  // namespace gf
+
+// ------------------------------------------------------------------ C ABI
 extern "C" {
 
 gf_status gf_precond_create(gf_assembler* a, int32_t fill_level, int32_t precision,
@@ -309,7 +1145,7 @@ gf_status gf_precond_create(gf_assembler* a, int32_t fill_level, int32_t precisi
   p->prec = precision;
   p->pat = fill_level == 0 ? a->pat : iluk_pattern(a->pat, fill_level);
   const int n = a->nnodes;
-  std::vector<int32_t> diag(n), lvL, lvU, ordL(n), ordU(n), amap(a->pat.nnz());
+  std::vector<int32_t> diag(n), amap(a->pat.nnz());
   for (int i = 0; i < n; i++) {
     const int32_t* b0 = p->pat.cols.data() + p->pat.rowp[i];
     const int32_t* b1 = p->pat.cols.data() + p->pat.rowp[i + 1];
@@ -319,11 +1155,8 @@ gf_status gf_precond_create(gf_assembler* a, int32_t fill_level, int32_t precisi
       amap[jp] = (int32_t)(f - p->pat.cols.data());
     }
   }
-  p->nlevL = levels(p->pat, true, lvL);
-  p->nlevU = levels(p->pat, false, lvU);
-  for (int i = 0; i < n; i++) ordL[i] = ordU[i] = i;
-  std::stable_sort(ordL.begin(), ordL.end(), [&](int x, int y) { return lvL[x] < lvL[y]; });
-  std::stable_sort(ordU.begin(), ordU.end(), [&](int x, int y) { return lvU[x] < lvU[y]; });
+  p->nlevL = levels(p->pat, true, p->lvL);
+  p->nlevU = levels(p->pat, false, p->lvU);
   cudaError_t e = cudaSuccess;
   auto up = [&](cudaError_t x) {
     if (e == cudaSuccess) e = x;
@@ -331,16 +1164,9 @@ gf_status gf_precond_create(gf_assembler* a, int32_t fill_level, int32_t precisi
   up(p->d_rowp.upload(p->pat.rowp));
   up(p->d_cols.upload(p->pat.cols));
   up(p->d_diag.upload(diag));
-  up(p->d_orderL.upload(ordL));
-  up(p->d_orderU.upload(ordU));
   up(p->d_amap.upload(amap));
-  up(p->d_flags.alloc(n));
-  if (e == cudaSuccess) up(cudaMemset(p->d_flags.p, 0, sizeof(int32_t) * n));
   up(p->d_lu.alloc((size_t)36 * p->pat.nnz()));
   if (precision == GF_PREC_FP32) up(p->d_lu32.alloc((size_t)36 * p->pat.nnz()));
-  up(p->d_tmp.alloc((size_t)6 * n));
-  up(p->d_ctl.alloc(1));
-  if (e == cudaSuccess) up(cudaMemset(p->d_ctl.p, 0, sizeof(SweepCtl)));
   if (e != cudaSuccess) {
     set_last_error("gf_precond_create", e);
     delete p;
@@ -351,6 +1177,7 @@ gf_status gf_precond_create(gf_assembler* a, int32_t fill_level, int32_t precisi
 }
 
 gf_status gf_precond_destroy(gf_precond* p) {
+  if (p && p->self) delete p->self;
   delete p;
   return GF_OK;
 }
@@ -374,107 +1201,135 @@ gf_status gf_precond_get(const gf_precond* p, int32_t* rowPtr, int32_t* colPtr,
   return GF_OK;
 }
 
-static int persistent_blocks() {
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  return sms * 8;
-}
-
 gf_status gf_precond_factor(gf_precond* p, gf_bsr* A, void* stream) {
   if (!p || !A || A->a != p->a) return GF_INVALID_ARG;
-  cudaStream_t st = as_stream(stream);
-  const int n = p->a->nnodes;
-  const size_t nv = (size_t)36 * p->pat.nnz();
-  GF_CUDA(cudaMemsetAsync(p->d_lu.p, 0, sizeof(double) * nv, st));
-  const size_t na = (size_t)36 * p->a->pat.nnz();
-  scatter_values_kernel<<<(unsigned)((na + 255) / 256), 256, 0, st>>>(p->a->pat.nnz(),
-                                                                      p->d_amap.p, A->vals.p,
-                                                                      p->d_lu.p);
-  GF_CHECK_LAUNCH();
-  GF_CUDA(cudaMemsetAsync(&p->d_ctl.p->status, 0, 2 * sizeof(int), st));
-  sweep_begin<<<1, 1, 0, st>>>(p->d_ctl.p);
-  GF_CHECK_LAUNCH();
-  const int nb = std::min(persistent_blocks(), (n + 3) / 4);
-  ilu_factor_kernel<<<nb, 128, 0, st>>>(n, p->d_rowp.p, p->d_cols.p, p->d_diag.p,
-                                        p->d_orderL.p, p->d_lu.p, p->d_flags.p, p->d_ctl.p);
-  GF_CHECK_LAUNCH();
-  if (p->prec == GF_PREC_FP32) {
-    convert_kernel<float><<<(unsigned)((nv + 255) / 256), 256, 0, st>>>(nv, p->d_lu.p,
-                                                                        p->d_lu32.p);
-    GF_CHECK_LAUNCH();
-  }
-  SweepCtl h;
-  GF_CUDA(cudaMemcpyAsync(&h, p->d_ctl.p, sizeof(SweepCtl), cudaMemcpyDeviceToHost, st));
-  GF_CUDA(cudaStreamSynchronize(st));
-  if (h.status & ST_TIMEOUT) return GF_TIMEOUT;
-  if (h.status & ST_ZERO_PIVOT) return GF_ZERO_PIVOT;
-  return GF_OK;
+  gf_status s = self_batch(p, A);
+  if (s != GF_OK) return s;
+  return batch_factor(p->self, as_stream(stream));
 }
 
 gf_status gf_precond_apply(gf_precond* p, const double* d_r, double* d_z, void* stream) {
-  if (!p || !d_r || !d_z) return GF_INVALID_ARG;
-  return precond_apply_impl(p, d_r, d_z, as_stream(stream));
+  if (!p || !d_r || !d_z || !p->self) return GF_INVALID_ARG;
+  cudaStream_t st = as_stream(stream);
+  gf_batch* B = p->self;
+  gf_status s = (p->prec == GF_PREC_FP32) ? bprecond<float>(B, nullptr, d_r, B->d_x.p, st)
+                                          : bprecond<double>(B, nullptr, d_r, B->d_x.p, st);
+  if (s != GF_OK) return s;
+  GF_CUDA(cudaMemcpyAsync(d_z, B->d_x.p, sizeof(double) * B->N, cudaMemcpyDeviceToDevice, st));
+  SweepCtl h;
+  s = read_ctl(B, st, &h);
+  if (s != GF_OK) return s;
+  return (h.status & ST_TIMEOUT) ? GF_TIMEOUT : GF_OK;
+}
+
+void gf_solve_opts_default(gf_solve_opts* o) {
+  if (!o) return;
+  o->restart = 50;
+  o->max_iters = 5000;
+  o->rtol = 1e-8;
+  o->side = 1;
+  o->mixed = 0;
+  o->inner_rtol = 1e-4;
+  o->max_refine = 30;
+  o->check_every = 25;
+}
+
+gf_status gf_batch_create(int32_t n, gf_assembler* const* asms, gf_bsr* const* mats,
+                          gf_precond* const* pcs, gf_batch** out) {
+  if (n <= 0 || !asms || !mats || !pcs || !out) return GF_INVALID_ARG;
+  for (int k = 0; k < n; k++)
+    if (!asms[k] || !mats[k] || !pcs[k] || mats[k]->a != asms[k] || pcs[k]->a != asms[k])
+      return GF_INVALID_ARG;
+  return batch_create_impl(n, asms, mats, pcs, out);
+}
+
+gf_status gf_batch_destroy(gf_batch* b) {
+  delete b;
+  return GF_OK;
+}
+
+gf_status gf_batch_assemble(gf_batch* B, void* stream) {
+  if (!B) return GF_INVALID_ARG;
+  for (int k = 0; k < B->np; k++) {
+    gf_status s = gf_add_jacobian(B->asms[k], nullptr, B->mats[k], GF_ASSEMBLE_FUSE_BCS, stream);
+    if (s != GF_OK) return s;
+  }
+  return GF_OK;
+}
+
+gf_status gf_batch_factor(gf_batch* B, void* stream) {
+  if (!B) return GF_INVALID_ARG;
+  return batch_factor(B, as_stream(stream));
+}
+
+gf_status gf_batch_solve(gf_batch* B, const double* const* d_b, double* const* d_x,
+                         const gf_solve_opts* opts, gf_solve_stats* stats, void* stream) {
+  if (!B || !d_b || !d_x) return GF_INVALID_ARG;
+  gf_solve_opts o;
+  gf_solve_opts_default(&o);
+  if (opts) o = *opts;
+  if (!opts_ok(o)) return GF_INVALID_ARG;
+  for (int k = 0; k < B->np; k++)
+    if (!d_b[k] || !d_x[k]) return GF_INVALID_ARG;
+  cudaStream_t st = as_stream(stream);
+  std::vector<PermEntry> eb(B->np), ex(B->np), eo(B->np);
+  int maxn = 0;
+  for (int k = 0; k < B->np; k++) {
+    gf_assembler* a = B->asms[k];
+    eb[k] = PermEntry{a->d_perm.p, a->nnodes, B->offs[k], d_b[k], B->d_b.p};
+    ex[k] = PermEntry{a->d_perm.p, a->nnodes, B->offs[k], d_x[k], B->d_x.p};
+    eo[k] = PermEntry{a->d_perm.p, a->nnodes, B->offs[k], B->d_x.p, d_x[k]};
+    maxn = std::max(maxn, a->nnodes);
+  }
+  GF_CUDA(cudaMemcpyAsync(B->d_perm_b.p, eb.data(), sizeof(PermEntry) * B->np,
+                          cudaMemcpyHostToDevice, st));
+  GF_CUDA(cudaMemcpyAsync(B->d_perm_x.p, ex.data(), sizeof(PermEntry) * B->np,
+                          cudaMemcpyHostToDevice, st));
+  GF_CUDA(cudaMemcpyAsync(B->d_perm_out.p, eo.data(), sizeof(PermEntry) * B->np,
+                          cudaMemcpyHostToDevice, st));
+  const dim3 grid((unsigned)std::max(1, std::min(64, (6 * maxn + 255) / 256)), (unsigned)B->np);
+  bpermute<<<grid, 256, 0, st>>>(B->d_perm_b.p, 0); ::gf::count_launch();
+  bpermute<<<grid, 256, 0, st>>>(B->d_perm_x.p, 0); ::gf::count_launch();
+  GF_CHECK_LAUNCH();
+  std::vector<gf_solve_stats> S;
+  gf_status s = batch_solve_space(B, o, S, st);
+  bpermute<<<grid, 256, 0, st>>>(B->d_perm_out.p, 1); ::gf::count_launch();
+  GF_CHECK_LAUNCH();
+  GF_CUDA(cudaStreamSynchronize(st));
+  if (stats)
+    for (int k = 0; k < B->np; k++) stats[k] = S[k];
+  return s;
+}
+
+gf_status gf_gmres_solve(gf_assembler* a, gf_bsr* A, gf_precond* p, const double* d_b,
+                         double* d_x, const gf_solve_opts* opts, gf_solve_stats* stats,
+                         void* stream) {
+  if (!a || !A || !p || !d_b || !d_x || A->a != a || p->a != a) return GF_INVALID_ARG;
+  gf_status s = self_batch(p, A);
+  if (s != GF_OK) return s;
+  return gf_batch_solve(p->self, &d_b, &d_x, opts, stats, stream);
+}
+
+gf_status gf_bsr_spmv(gf_bsr* m, double alpha, const double* d_x, double beta, double* d_y,
+                      void* stream) {
+  if (!m || !d_x || !d_y) return GF_INVALID_ARG;
+  gf_assembler* a = m->a;
+  cudaStream_t st = as_stream(stream);
+  if (!m->desc.p) {
+    ProbDev d{};
+    d.n = a->nnodes;
+    d.off = 0;
+    d.rowp = a->d_rowp.p;
+    d.cols = a->d_cols.p;
+    d.A64 = m->vals.p;
+    GF_CUDA(m->desc.upload(&d, 1));
+    GF_CUDA(m->rowprob.alloc(a->nnodes));
+    GF_CUDA(cudaMemset(m->rowprob.p, 0, sizeof(int32_t) * a->nnodes));
+  }
+  bspmv_kernel<double><<<(a->nnodes + 7) / 8, 256, 0, st>>>(a->nnodes, m->rowprob.p, m->desc.p,
+                                                            nullptr, d_x, alpha, beta, d_y); ::gf::count_launch();
+  GF_CHECK_LAUNCH();
+  return GF_OK;
 }
 
 }  // extern "C"
-
-namespace gf {
-
-gf_status precond_apply_impl(gf_precond* p, const double* r, double* z, cudaStream_t st) {
-  const int n = p->a->nnodes;
-  const int nb = std::min(persistent_blocks(), (n + 3) / 4);
-  sweep_begin<<<1, 1, 0, st>>>(p->d_ctl.p);
-  if (p->prec == GF_PREC_FP32) {
-    trisolve_kernel<float, false><<<nb, 128, 0, st>>>(n, p->d_rowp.p, p->d_cols.p, p->d_diag.p,
-                                                      p->d_orderL.p, p->d_lu32.p, r,
-                                                      p->d_tmp.p, p->d_flags.p, p->d_ctl.p);
-    sweep_begin<<<1, 1, 0, st>>>(p->d_ctl.p);
-    trisolve_kernel<float, true><<<nb, 128, 0, st>>>(n, p->d_rowp.p, p->d_cols.p, p->d_diag.p,
-                                                     p->d_orderU.p, p->d_lu32.p, p->d_tmp.p, z,
-                                                     p->d_flags.p, p->d_ctl.p);
-  } else {
-    trisolve_kernel<double, false><<<nb, 128, 0, st>>>(n, p->d_rowp.p, p->d_cols.p, p->d_diag.p,
-                                                       p->d_orderL.p, p->d_lu.p, r, p->d_tmp.p,
-                                                       p->d_flags.p, p->d_ctl.p);
-    sweep_begin<<<1, 1, 0, st>>>(p->d_ctl.p);
-    trisolve_kernel<double, true><<<nb, 128, 0, st>>>(n, p->d_rowp.p, p->d_cols.p, p->d_diag.p,
-                                                      p->d_orderU.p, p->d_lu.p, p->d_tmp.p, z,
-                                                      p->d_flags.p, p->d_ctl.p);
-  }
-  GF_CHECK_LAUNCH();
-  return GF_OK;
-}
-
-template <class VT>
-gf_status spmv_impl(int n, const int32_t* rowp, const int32_t* cols, const VT* A,
-                    const double* x, double alpha, double beta, double* y, cudaStream_t st) {
-  const int threads = 256, rows_per_block = threads / 32;
-  spmv_kernel<VT><<<(n + rows_per_block - 1) / rows_per_block, threads, 0, st>>>(
-      n, rowp, cols, A, x, alpha, beta, y);
-  GF_CHECK_LAUNCH();
-  return GF_OK;
-}
-template gf_status spmv_impl<double>(int, const int32_t*, const int32_t*, const double*,
-                                     const double*, double, double, double*, cudaStream_t);
-template gf_status spmv_impl<float>(int, const int32_t*, const int32_t*, const float*,
-                                    const double*, double, double, double*, cudaStream_t);
-
-gf_status precond_status(gf_precond* p, cudaStream_t st, int* bits) {
-  SweepCtl h;
-  GF_CUDA(cudaMemcpyAsync(&h, p->d_ctl.p, sizeof(SweepCtl), cudaMemcpyDeviceToHost, st));
-  GF_CUDA(cudaStreamSynchronize(st));
-  *bits = h.status;
-  return GF_OK;
-}
-
-int* precond_status_ptr(gf_precond* p) { return &p->d_ctl.p->status; }
-
-}  // namespace gf
-
-extern "C" gf_status gf_bsr_spmv(gf_bsr* m, double alpha, const double* d_x, double beta,
-                                 double* d_y, void* stream) {
-  if (!m || !d_x || !d_y) return GF_INVALID_ARG;
-  return spmv_impl<double>(m->a->nnodes, m->a->d_rowp.p, m->a->d_cols.p, m->vals.p, d_x, alpha,
-                           beta, d_y, as_stream(stream));
-}

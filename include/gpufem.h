@@ -73,12 +73,15 @@ enum { GF_ASSEMBLE_OVERWRITE = 0, GF_ASSEMBLE_ADD = 1, GF_ASSEMBLE_FUSE_BCS = 2 
 typedef struct gf_assembler gf_assembler;
 typedef struct gf_bsr gf_bsr;
 typedef struct gf_precond gf_precond;
+typedef struct gf_batch gf_batch;
 
 /* ---- library --------------------------------------------------------- */
 const char* gf_status_string(gf_status s);
 const char* gf_version(void);
 /* Last CUDA error text seen by the library on this thread ("" if none). */
 const char* gf_last_error(void);
+/* Number of kernels the library has launched in this process (all threads). */
+long long gf_launch_count(void);
 
 /* ---- assembler ------------------------------------------------------- */
 /* ElementAssembler(...) (include/assembler.h:31-73) + BsrData(...)
@@ -108,6 +111,10 @@ gf_status gf_assembler_get_schedule(const gf_assembler* a, int32_t* elem_chunk,
 /* set_variables (include/assembler.h:191-195): d_vars is natural-order,
  * 6*num_nodes doubles on the device; copied (not referenced). */
 gf_status gf_set_variables(gf_assembler* a, const double* d_vars, void* stream);
+/* Replace the per-element thickness (device pointer, natural element order,
+ * num_elements doubles); other material data is kept. Lets one assembler
+ * (pattern, ordering, schedule) serve many thickness fields on one mesh. */
+gf_status gf_assembler_set_thickness(gf_assembler* a, const double* d_thick, void* stream);
 /* add_residual (include/assembler.h:232-264, kernel base/elem_group.cuh:17-97):
  * d_res (natural order) = R(u)  (or += with GF_ASSEMBLE_ADD). */
 gf_status gf_add_residual(gf_assembler* a, double* d_res, int32_t flags, void* stream);
@@ -196,6 +203,26 @@ void gf_solve_opts_default(gf_solve_opts* o);
 gf_status gf_gmres_solve(gf_assembler* a, gf_bsr* A, gf_precond* p, const double* d_b,
                          double* d_x, const gf_solve_opts* opts, gf_solve_stats* stats,
                          void* stream);
+
+/* ---- batched uneven solves ------------------------------------------- */
+/* A batch of independent problems (assembler + BSR matrix + preconditioner
+ * each) solved together: SpMV, ILU factorization and both triangular sweeps
+ * run as one launch over the whole batch (merged level order), GMRES keeps
+ * per-problem Arnoldi states and per-problem reductions, so every problem's
+ * result is bitwise the same alone and in any batch. No reference
+ * counterpart: the reference solves one problem per driver
+ * (examples/iterative/gmres.cu). The handles must outlive the batch. */
+gf_status gf_batch_create(int32_t n, gf_assembler* const* asms, gf_bsr* const* mats,
+                          gf_precond* const* pcs, gf_batch** out);
+gf_status gf_batch_destroy(gf_batch* b);
+/* add_jacobian with fused BCs for every problem. */
+gf_status gf_batch_assemble(gf_batch* b, void* stream);
+/* Numeric ILU(k) of every problem in one level-ordered launch. */
+gf_status gf_batch_factor(gf_batch* b, void* stream);
+/* Solve every problem: d_b[k], d_x[k] device pointers (natural order,
+ * d_x[k] is the initial guess); stats[k] per problem (may be NULL). */
+gf_status gf_batch_solve(gf_batch* b, const double* const* d_b, double* const* d_x,
+                         const gf_solve_opts* opts, gf_solve_stats* stats, void* stream);
 
 #ifdef __cplusplus
 }
