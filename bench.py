@@ -339,7 +339,7 @@ def main():
         "mixed_over_fp64": ms_fp64 / ms_mixed,
         "e2e": {"value": ws * nprob / (ms_e2e / 1e3), "unit": "solves/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
-        "roofline": {"kernel": "trisolve_kernel (block L and U sweeps, FP32 values)",
+        "roofline": {"kernel": "bsweep_tma (block L and U sweeps, FP32 values)",
                      "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": None, "levels": [inf["levels_L"], inf["levels_U"]],

@@ -78,6 +78,7 @@ SIGNATURES = {
     "gf_assembler_set_thickness": (_I, [_P, _P, _P]),
     "gf_add_residual": (_I, [_P, _P, _I, _P]),
     "gf_add_jacobian": (_I, [_P, _P, _P, _I, _P]),
+    "gf_add_jacobian_thick": (_I, [_P, _P, _P, _P, _I, _P]),
     "gf_add_energy": (_I, [_P, _PD, _P]),
     "gf_apply_bcs_vec": (_I, [_P, _P, _P]),
     "gf_apply_bcs_mat": (_I, [_P, _P, _P]),
@@ -99,6 +100,7 @@ SIGNATURES = {
     "gf_batch_create": (_I, [_I, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]),
     "gf_batch_destroy": (_I, [_P]),
     "gf_batch_assemble": (_I, [_P, _P]),
+    "gf_batch_assemble_ex": (_I, [_P, C.POINTER(_P), _P]),
     "gf_batch_factor": (_I, [_P, _P]),
     "gf_batch_solve": (_I, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(gf_solve_opts),
                             C.POINTER(gf_solve_stats), _P]),

@@ -76,7 +76,8 @@ def solve_opts(rtol=1e-8, mixed=False, restart=100, max_iters=20000, inner_rtol=
 class BatchSolver:
     """Problems resident on the current device, solved as one batch."""
 
-    def __init__(self, meshes, ordering="rcm", tune=True, fill=None, rtol=1e-8, restart=100):
+    def __init__(self, meshes, ordering="rcm", tune=True, fill=None, rtol=1e-8, restart=100,
+                 build=True):
         self.rtol, self.restart = rtol, restart
         self.meshes = meshes
         self.asms = [ElementAssembler.from_mesh(m, ordering=ordering) for m in meshes]
@@ -93,6 +94,8 @@ class BatchSolver:
             self.fills, self.tune_log = self._autotune()
         else:
             self.fills, self.tune_log = [0] * n, None
+        if not build:  # fill levels only (the server tunes its size classes this way)
+            return
         self.P64 = [ILUk_Preconditioner(a, k, "fp64") for a, k in zip(self.asms, self.fills)]
         self.P32 = [ILUk_Preconditioner(a, k, "fp32") for a, k in zip(self.asms, self.fills)]
         self.b64 = Batch(self.asms, self.mats, self.P64)

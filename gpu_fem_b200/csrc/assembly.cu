@@ -5,8 +5,8 @@
 // scatter with FP64 atomicAdd (include/linalg/vec.h:278-293,
 // include/linalg/bsr_mat.h:229-276).
 //
-// Here a warp works on batches of up to eight elements:
-//   * coordinates and DOFs of the batch are gathered into the warp's shared
+// Here a warp owns a chunk of up to eight neighbouring elements:
+//   * coordinates and DOFs of the chunk are gathered into the warp's shared
 //     memory slot and the per-element geometry (normals, nodal frames, the
 //     four quadrature-point frames, the tying-point vectors) is computed by
 //     8 x 4 lanes at once;
@@ -14,20 +14,20 @@
 //     matrices B_q and of D B_q; each of the 32 lanes then owns a 3x6 tile of
 //     K_e = sum_q B_q^T D B_q (144 contiguous bytes of one 6x6 BSR block) and
 //     writes it with 16-byte stores; R_e = K_e u_e follows from the tiles;
-//   * the scatter follows the coloured schedule built on the host: one CTA
-//     per chunk, chunks of one colour per launch, element colours separated
-//     by __syncthreads(). The first toucher of a block stores, later touchers
-//     read-modify-write; there are no atomics and the result is bitwise
-//     reproducible.
+//   * the scatter follows the coloured schedule built on the host: chunks of
+//     one colour share no node and run concurrently (one launch per colour);
+//     inside a chunk the warp handles its elements in order. The first
+//     toucher of a block stores, later touchers read-modify-write; there are
+//     no atomics and the result is bitwise reproducible.
 #include <cstdio>
 
 #include "gf_internal.h"
 
 namespace gf {
 
-constexpr int kAsmWarps = 4;
-constexpr int kEPW = 8;          // elements per warp batch (geometry spread over 8 x 4 lanes)
-constexpr int kChunkSize = 128;  // elements per chunk (one CTA per chunk)
+constexpr int kAsmWarps = 2;     // warps (= chunks) per CTA
+constexpr int kEPW = 8;          // elements per chunk; geometry spread over 8 x 4 lanes
+constexpr int kChunkSize = kEPW;
 
 struct WarpSlot {
   double X[kEPW][12];
@@ -50,8 +50,9 @@ struct AsmParams {
   const int32_t* smat;
   const Material* mats;
   const int32_t* chunk_start;
-  const int32_t* ec_off;
-  int chunk_base;
+  const double* thick_nat;   // optional per-call thickness (natural element order)
+  const int32_t* sorder;     // schedule position -> element
+  int chunk_base, chunk_end;
   double* values;
   double* res;
   double* energy_part;
@@ -92,7 +93,7 @@ template <int MODE>
 __device__ void process_element(int s, int k, WarpSlot& w, const AsmParams& P, int lane,
                                 double& energy_acc) {
   const Material m = P.mats[P.smat ? P.smat[s] : 0];
-  const double t = P.sthick[s];
+  const double t = P.thick_nat ? P.thick_nat[P.sorder[s]] : P.sthick[s];
   const ElemGeom& g = w.g[k];
   if (lane < 24) {
     double Bc[36];
@@ -237,31 +238,14 @@ __global__ void __launch_bounds__(kAsmWarps * 32)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   WarpSlot* slots = reinterpret_cast<WarpSlot*>(smem_raw);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int li = P.chunk_base + blockIdx.x;
-  const int s0 = P.chunk_start[li];
-  const int32_t* off = &P.ec_off[(size_t)li * (kMaxEC + 1)];
-  double energy_acc = 0.0;
+  const int li = P.chunk_base + blockIdx.x * kAsmWarps + warp;  // this warp's chunk
+  if (li >= P.chunk_end) return;
+  const int s0 = P.chunk_start[li], cnt = P.chunk_start[li + 1] - s0;
   WarpSlot& w = slots[warp];
-  for (int col = 0; col < kMaxEC; col++) {
-    const int b = off[col], e = off[col + 1];
-    if (b == e) continue;
-    for (int base = b + warp * kEPW; base < e; base += kAsmWarps * kEPW) {
-      const int cnt = min(kEPW, e - base);
-      batch_geometry(s0 + base, cnt, w, P, lane);
-      for (int k = 0; k < cnt; k++) process_element<MODE>(s0 + base + k, k, w, P, lane, energy_acc);
-    }
-    __syncthreads();
-  }
-  if (MODE == MODE_ENERGY) {
-    __shared__ double part[kAsmWarps];
-    if (lane == 0) part[warp] = energy_acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double sum = 0.0;
-      for (int w2 = 0; w2 < kAsmWarps; w2++) sum += part[w2];
-      P.energy_part[li] = sum;
-    }
-  }
+  double energy_acc = 0.0;
+  batch_geometry(s0, cnt, w, P, lane);
+  for (int k = 0; k < cnt; k++) process_element<MODE>(s0 + k, k, w, P, lane, energy_acc);
+  if (MODE == MODE_ENERGY && lane == 0) P.energy_part[li] = energy_acc;
 }
 
 __global__ void sum_kernel(const double* part, int n, double* out) {
@@ -318,7 +302,7 @@ __global__ void permute_kernel(const int32_t* perm, int nnodes, const double* in
 
 template <int MODE>
 static gf_status launch_assembly(gf_assembler* a, double* values, double* res, int flags,
-                                 cudaStream_t st) {
+                                 cudaStream_t st, const double* thick_nat = nullptr) {
   AsmParams P;
   P.xpts = a->d_xpts.p;
   P.vars = a->d_vars.p;
@@ -330,23 +314,23 @@ static gf_status launch_assembly(gf_assembler* a, double* values, double* res, i
   P.smat = a->d_smat.p;
   P.mats = a->d_mats.p;
   P.chunk_start = a->d_chunk_start.p;
-  P.ec_off = a->d_ec_off.p;
+  P.thick_nat = thick_nat;
+  P.sorder = a->d_sorder.p;
   P.values = values;
   P.res = res;
   P.energy_part = a->d_energy_part.p;
   P.flags = flags;
   const size_t smem = sizeof(WarpSlot) * kAsmWarps;
-  static bool attr_set[3] = {false, false, false};
-  if (!attr_set[MODE]) {
-    GF_CUDA(cudaFuncSetAttribute(assemble_kernel<MODE>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr_set[MODE] = true;
-  }
+  // per device and constant, so setting it on every call is race-free
+  GF_CUDA(cudaFuncSetAttribute(assemble_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem));
   const Schedule& s = a->sched;
   for (int cc = 0; cc < s.ncc; cc++) {
-    const int nblk = s.cc_start[cc + 1] - s.cc_start[cc];
-    if (nblk == 0) continue;
+    const int nch = s.cc_start[cc + 1] - s.cc_start[cc];
+    if (nch == 0) continue;
+    const int nblk = (nch + kAsmWarps - 1) / kAsmWarps;
     P.chunk_base = s.cc_start[cc];
+    P.chunk_end = s.cc_start[cc + 1];
     assemble_kernel<MODE><<<nblk, kAsmWarps * 32, smem, st>>>(P); ::gf::count_launch();
     GF_CHECK_LAUNCH();
   }
@@ -477,7 +461,6 @@ gf_status gf_assembler_create(const gf_mesh_desc* d, gf_assembler** out) {
   up(a->d_sthick.upload(sthick));
   up(a->d_sorder.upload(s.order));
   up(a->d_chunk_start.upload(s.chunk_start));
-  up(a->d_ec_off.upload(s.ec_off));
   up(a->d_mats.upload(a->mats));
   up(a->d_rowp.upload(P.rowp));
   up(a->d_cols.upload(P.cols));
@@ -543,6 +526,12 @@ gf_status gf_add_jacobian(gf_assembler* a, double* d_res, gf_bsr* mat, int32_t f
                           void* stream) {
   if (!a || !mat || mat->a != a) return GF_INVALID_ARG;
   return launch_assembly<MODE_JAC>(a, mat->vals.p, d_res, flags, as_stream(stream));
+}
+
+gf_status gf_add_jacobian_thick(gf_assembler* a, const double* d_thick, double* d_res,
+                                gf_bsr* mat, int32_t flags, void* stream) {
+  if (!a || !mat || mat->a != a || !d_thick) return GF_INVALID_ARG;
+  return launch_assembly<MODE_JAC>(a, mat->vals.p, d_res, flags, as_stream(stream), d_thick);
 }
 
 gf_status gf_add_energy(gf_assembler* a, double* h_energy, void* stream) {

@@ -97,14 +97,32 @@ struct Schedule {
   std::vector<int32_t> chunk_list;    // chunks sorted by (colour, id)
   std::vector<int32_t> cc_start;      // [ncc+1] offsets into chunk_list
   std::vector<int32_t> chunk_start;   // [nchunks+1] schedule offsets (in chunk_list order)
-  std::vector<int32_t> ec_off;        // [nchunks * (kMaxEC+1)] colour offsets within chunk
 };
 constexpr int kMaxEC = 15;
 
+// Level-major chunk stream of one triangle (L or U) of a block ILU factor.
+// Rows are grouped by level and cut into chunks (a chunk never spans two
+// levels; at most capb blocks and capr rows). Chunk c is one contiguous,
+// 16-byte aligned byte range [off[c], off[c+1]) of `stream`:
+//   int4 header {nrows, nblocks, 0, 0}
+//   nrows x int4 {row, first block (chunk-local), blocks, 0}
+//   nblocks x int32 column (problem-local block row)
+//   nblocks x 36 values (row-major 6x6, factor precision)
+// so one bulk copy brings everything a chunk's solve needs into shared
+// memory. nblocks is a non-zero multiple of 4 (zero padding blocks). For U
+// every row starts with its U_ii^{-1} block.
+struct TriDesc {
+  int nch;                       // chunks
+  int stage;                     // bytes of the largest chunk (staging buffer size)
+  int capb, capr;                // blocks / rows per chunk at most
+  const int64_t* off;            // [nch+1] byte offsets into stream
+  const unsigned char* stream;
+};
+
 // Per-problem descriptor used by the batched solver kernels: block rows,
 // offset of the problem in the batch vector space (in block rows), the
-// matrix pattern and values (FP64 and the FP32 copy of the mixed mode), and
-// the ILU pattern and factor values.
+// matrix pattern and values (FP64 and the FP32 copy of the mixed mode), the
+// ILU pattern and factor values, and the factor's chunk streams.
 struct ProbDev {
   int n, off;
   const int32_t* rowp;
@@ -114,8 +132,11 @@ struct ProbDev {
   const int32_t* prowp;
   const int32_t* pcols;
   const int32_t* pdiag;
-  double* LU64;
-  float* LU32;
+  double* LU64;              // factor in ILU-pattern order (FP64)
+  int nlevL, nlevU;          // triangular levels
+  const int32_t* levLptr;    // rows grouped by lower level (factorization order)
+  const int32_t* levLrows;
+  TriDesc L, U;              // chunk streams of the factor for the sweeps
 };
 int build_schedule(int nelem, int nnodes, const int32_t* conn, const std::vector<int32_t>& emap,
                    int nnzb, int chunk_size, Schedule& s);
@@ -142,7 +163,7 @@ struct gf_assembler {
   gf::DevBuf<uint32_t> d_sft;
   gf::DevBuf<double> d_sthick;
   gf::DevBuf<int32_t> d_sorder;     // schedule position -> element
-  gf::DevBuf<int32_t> d_chunk_list, d_chunk_start, d_ec_off;
+  gf::DevBuf<int32_t> d_chunk_list, d_chunk_start;
   gf::DevBuf<gf::Material> d_mats;
   // device: pattern (solver order) and BC entry list
   gf::DevBuf<int32_t> d_rowp, d_cols;

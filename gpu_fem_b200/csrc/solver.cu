@@ -9,17 +9,14 @@
 //
 // Batch layout: every problem keeps its own pattern / values / factor
 // buffers; a device table of ProbDev descriptors gives each kernel the
-// problem of a global block row (row_prob) and its offset in the batch vector
-// space. Triangular work (factorization, L and U sweeps) runs as one
-// persistent launch per sweep over the merged level order of all problems:
-// warps take rows from an atomic counter in that order, so every row a warp
-// waits for was taken earlier by a running warp and a sweep cannot deadlock.
-//  * factorization: per-row ready flags carrying an epoch;
-//  * sweeps: the output vector is pre-filled with a signalling-NaN sentinel
-//    that arithmetic never produces; a consumer polls the producer's six
-//    values directly (one L2 round trip, no flag or fence on the path).
-// Every wait is bounded (2 s of %globaltimer); a wait that runs out sets an
-// error bit in the status word and the launch ends instead of hanging.
+// problem of a global block row (row_prob), its offset in the batch vector
+// space and its triangular level structure.
+//  * SpMV and the GMRES vector work run over all rows / chunks of the batch.
+//  * Triangular work (the factorization and both sweeps) runs one CTA per
+//    problem: the CTA walks the problem's levels and separates them with
+//    __syncthreads(), so a dependency costs a block barrier (tens of ns)
+//    instead of a device-wide round trip; the problems of a batch run on
+//    different SMs at once.
 //
 // GMRES reductions are segmented per problem over fixed 4096-entry chunks
 // aligned to each problem's own vector, with per-problem Arnoldi states, so
@@ -35,9 +32,8 @@
 
 namespace gf {
 
-constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s per wait
 enum { ST_TIMEOUT = 1, ST_ZERO_PIVOT = 2, ST_NAN = 4 };
-constexpr unsigned long long kSentinel = 0x7FF4DEADBEEF0000ull;  // signalling-NaN payload
+constexpr int kCtaThreads = 1024;  // one CTA per problem for triangular work
 constexpr int kChunk = 4096;
 constexpr int kRedThreads = 256;
 
@@ -47,48 +43,6 @@ struct SweepCtl {
   int status;
   int pivot;
 };
-
-__device__ __forceinline__ bool is_sentinel(double v) {
-  return (unsigned long long)__double_as_longlong(v) == kSentinel;
-}
-__device__ __forceinline__ unsigned long long global_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-// Coherent (gpu-scope) load of a value another SM may be writing.
-__device__ __forceinline__ double ld_relaxed(const double* p) {
-  double v;
-  asm volatile("ld.relaxed.gpu.global.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void st_relaxed(double* p, double v) {
-  asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
-}
-// Bounded-wait helper: true once more than kWaitLimitNs has passed since t0.
-__device__ __forceinline__ bool wait_expired(unsigned long long t0, unsigned& polls) {
-  if ((++polls & 63u) != 0u) return false;
-  return global_ns() - t0 > kWaitLimitNs;
-}
-__device__ __forceinline__ int ld_acquire(const int* p) {
-  int v;
-  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void st_release(int* p, int v) {
-  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-
-__global__ void sweep_begin(SweepCtl* c) {
-  c->epoch += 1;
-  c->counter = 0;
-}
-__global__ void fill_sentinel(double* v, size_t n) {
-  const double s = __longlong_as_double((long long)kSentinel);
-  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
-       t += (size_t)gridDim.x * blockDim.x)
-    v[t] = s;
-}
 
 // ------------------------------------------------------------------ SpMV
 // y = alpha A x + beta y over all rows of live problems; one warp per block
@@ -177,95 +131,72 @@ __device__ void inv6_warp(double* M, double* Inv, int lane, SweepCtl* ctl, int r
 
 // IKJ block ILU on each problem's ILU pattern (FP64, in place): lower blocks
 // become L_ik = A_ik U_kk^{-1}, the diagonal block is replaced by U_ii^{-1}.
-__global__ void __launch_bounds__(128) bfactor_kernel(int nrows, const int32_t* __restrict__ row_prob,
-                                                      const ProbDev* __restrict__ P,
-                                                      const int32_t* __restrict__ order,
-                                                      int* flags, SweepCtl* ctl) {
-  __shared__ double sm[4][3][36];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+// One CTA per problem walks the levels of the lower-triangular DAG; the
+// rows of a level are independent and spread over the warps, and levels are
+// separated by __syncthreads() (block-scope visibility of global writes).
+__global__ void __launch_bounds__(kCtaThreads) bfactor_cta(const ProbDev* __restrict__ P,
+                                                          SweepCtl* ctl) {
+  __shared__ double sm[kCtaThreads / 32][3][36];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   double* Lb = sm[warp][0];
   double* M = sm[warp][1];
   double* Inv = sm[warp][2];
-  const int epoch = ctl->epoch;
-  while (true) {
-    int idx = 0;
-    if (lane == 0) idx = atomicAdd(&ctl->counter, 1);
-    idx = __shfl_sync(0xffffffffu, idx, 0);
-    if (idx >= nrows) break;
-    const int grow = order[idx];
-    const int p = row_prob[grow];
-    const ProbDev& d = P[p];
-    const int i = grow - d.off;
-    const int32_t* rowp = d.prowp;
-    const int32_t* cols = d.pcols;
-    const int32_t* diag = d.pdiag;
-    double* LU = d.LU64;
-    const int r0 = rowp[i], r1 = rowp[i + 1], di = diag[i];
-    // wait for every lower dependency, polled in parallel by the lanes
-    bool timed_out = false;
-    for (int base = r0; base < di; base += 32) {
-      const int kp = base + lane;
-      if (kp < di) {
-        const int* f = &flags[d.off + cols[kp]];
-        const unsigned long long t0 = global_ns();
-        unsigned polls = 0;
-        while (ld_acquire(f) != epoch) {
-          if (wait_expired(t0, polls)) {
-            timed_out = true;
-            break;
-          }
-          __nanosleep(32);
-        }
-      }
-    }
-    if (timed_out) atomicOr(&ctl->status, ST_TIMEOUT);
-    __syncwarp();
-    for (int kp = r0; kp < di; kp++) {
-      const int k = cols[kp];
-      const double* Ukk = LU + 36 * (size_t)diag[k];
-      const double* Aik = LU + 36 * (size_t)kp;
-      for (int t = lane; t < 36; t += 32) {
-        const int r = t / 6, c = t % 6;
-        double s = 0.0;
-#pragma unroll
-        for (int m = 0; m < 6; m++) s = fma(__ldcg(&Aik[6 * r + m]), __ldcg(&Ukk[6 * m + c]), s);
-        Lb[t] = s;
-      }
-      __syncwarp();
-      for (int t = lane; t < 36; t += 32) __stcg(&LU[36 * (size_t)kp + t], Lb[t]);
-      int tp = kp + 1;
-      const int k1 = rowp[k + 1];
-      for (int jp = diag[k] + 1; jp < k1; jp++) {
-        const int j = cols[jp];
-        while (tp < r1 && cols[tp] < j) tp++;
-        if (tp >= r1) break;
-        if (cols[tp] != j) continue;
-        const double* Ukj = LU + 36 * (size_t)jp;
-        double* Aij = LU + 36 * (size_t)tp;
+  const ProbDev d = P[blockIdx.x];
+  const int32_t* rowp = d.prowp;
+  const int32_t* cols = d.pcols;
+  const int32_t* diag = d.pdiag;
+  double* LU = d.LU64;
+  for (int lev = 0; lev < d.nlevL; lev++) {
+    for (int idx = d.levLptr[lev] + warp; idx < d.levLptr[lev + 1]; idx += nw) {
+      const int i = d.levLrows[idx];
+      const int r1 = rowp[i + 1], di = diag[i];
+      for (int kp = rowp[i]; kp < di; kp++) {
+        const int k = cols[kp];
+        const double* Ukk = LU + 36 * (size_t)diag[k];
+        const double* Aik = LU + 36 * (size_t)kp;
         for (int t = lane; t < 36; t += 32) {
           const int r = t / 6, c = t % 6;
           double s = 0.0;
 #pragma unroll
-          for (int m = 0; m < 6; m++) s = fma(Lb[6 * r + m], __ldcg(&Ukj[6 * m + c]), s);
-          __stcg(&Aij[t], __ldcg(&Aij[t]) - s);
+          for (int m = 0; m < 6; m++) s = fma(Aik[6 * r + m], Ukk[6 * m + c], s);
+          Lb[t] = s;
         }
+        __syncwarp();
+        for (int t = lane; t < 36; t += 32) LU[36 * (size_t)kp + t] = Lb[t];
+        int tp = kp + 1;
+        const int k1 = rowp[k + 1];
+        for (int jp = diag[k] + 1; jp < k1; jp++) {
+          const int j = cols[jp];
+          while (tp < r1 && cols[tp] < j) tp++;
+          if (tp >= r1) break;
+          if (cols[tp] != j) continue;
+          const double* Ukj = LU + 36 * (size_t)jp;
+          double* Aij = LU + 36 * (size_t)tp;
+          for (int t = lane; t < 36; t += 32) {
+            const int r = t / 6, c = t % 6;
+            double s = 0.0;
+#pragma unroll
+            for (int m = 0; m < 6; m++) s = fma(Lb[6 * r + m], Ukj[6 * m + c], s);
+            Aij[t] -= s;
+          }
+        }
+        __syncwarp();
+      }
+      double* Dii = LU + 36 * (size_t)di;
+      for (int t = lane; t < 36; t += 32) M[t] = Dii[t];
+      __syncwarp();
+      inv6_warp(M, Inv, lane, ctl, d.off + i);
+      for (int t = lane; t < 36; t += 32) {
+        const double v = Inv[t];
+        if (!isfinite(v)) {
+          atomicOr(&ctl->status, ST_ZERO_PIVOT);
+          atomicCAS(&ctl->pivot, 0, d.off + i + 1);
+        }
+        Dii[t] = v;
       }
       __syncwarp();
     }
-    double* Dii = LU + 36 * (size_t)di;
-    for (int t = lane; t < 36; t += 32) M[t] = __ldcg(&Dii[t]);
-    __syncwarp();
-    inv6_warp(M, Inv, lane, ctl, grow);
-    for (int t = lane; t < 36; t += 32) {
-      const double v = Inv[t];
-      if (!isfinite(v)) {
-        atomicOr(&ctl->status, ST_ZERO_PIVOT);
-        atomicCAS(&ctl->pivot, 0, grow + 1);
-      }
-      __stcg(&Dii[t], v);
-    }
-    __syncwarp();
-    if (lane == 0) st_release(&flags[grow], epoch);
+    __syncthreads();
   }
 }
 
@@ -281,80 +212,207 @@ __global__ void convert_kernel(size_t n, const double* __restrict__ in, T2* __re
   if (t < n) out[t] = (T2)in[t];
 }
 
-// --------------------------------------------------------- triangular sweeps
-// Lower: y_i = r_i - sum_{k<i} L_ik y_k. Upper: x_i = Uinv_ii (y_i - sum_{j>i} U_ij x_j).
-// `out` must hold the sentinel for every row of a live problem on entry.
+
+// ------------------------------------------- prefetched level-major sweeps
+// One CTA per problem walks the chunks of one triangle in level-major order.
+// A ring of kStages shared-memory buffers is filled by 1D bulk copies
+// (cp.async.bulk, completion counted on an mbarrier) kStages-1 chunks ahead
+// of the chunk being solved, so the HBM latency of the factor values is off
+// the critical path. Per chunk: wait for its stage, gather the x entries its
+// blocks multiply into shared memory (one parallel round of loads), then
+// solve its rows, spread over the warps (a chunk never spans two levels).
+// x / y live in global memory, written and re-read by this CTA only; two
+// block barriers per chunk order the gather after the previous chunk's
+// writes and the solve after the gather.
+constexpr int kSweepThreads = 512;
+constexpr int kStages = 3;
+constexpr unsigned long long kWaitNs = 2000000000ull;
+constexpr size_t kSweepSmemMax = 220 * 1024;  // dynamic; the static part is < 1 KB
+constexpr int kGather = 8;  // gathered values per thread and chunk: 6 (capb + capr) <= 4096
+
+__device__ __forceinline__ unsigned long long gtimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait; returns false if kWaitNs passed first
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+  const unsigned long long t0 = gtimer();
+  unsigned n = 0;
+  while (!mbar_try_wait(bar, parity)) {
+    if ((++n & 255u) == 0u && gtimer() - t0 > kWaitNs) return false;
+  }
+  return true;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes,
+                                         uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Dynamic shared memory of one sweep: kStages staging buffers of `stage`
+// bytes, then the gathered x of one chunk (capb x 6 doubles) and its
+// right-hand sides (capr x 6 doubles).
+__host__ __device__ inline size_t sweep_smem_bytes(int stage, int capb, int capr) {
+  return kStages * (size_t)stage + 48 * ((size_t)capb + capr);
+}
+
 template <class VT, bool UPPER>
-__global__ void __launch_bounds__(128) bsweep_kernel(int nrows, const int32_t* __restrict__ row_prob,
-                                                     const ProbDev* __restrict__ P,
-                                                     const int* __restrict__ live,
-                                                     const int32_t* __restrict__ order,
-                                                     const double* __restrict__ rhs, double* out,
-                                                     SweepCtl* ctl) {
-  const int lane = threadIdx.x & 31;
+__global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __restrict__ P,
+                                                           const int* __restrict__ live,
+                                                           const double* __restrict__ rhs,
+                                                           double* out, SweepCtl* ctl) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ uint64_t bar[kStages];
+  __shared__ int abort_flag;
+  const int p = blockIdx.x;
+  if (live && !live[p]) return;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
   const int g = lane / 6, r = lane % 6;
-  int next = 0;
-  if (lane == 0) next = atomicAdd(&ctl->counter, 1);
-  next = __shfl_sync(0xffffffffu, next, 0);
-  bool timed_out = false;
-  while (next < nrows) {
-    const int idx = next;
-    if (lane == 0) next = atomicAdd(&ctl->counter, 1);  // prefetch the next row index
-    next = __shfl_sync(0xffffffffu, next, 0);
-    const int grow = order[idx];
-    const int p = row_prob[grow];
-    if (live && !live[p]) continue;
-    const ProbDev& d = P[p];
-    const int i = grow - d.off;
-    const VT* LU = sizeof(VT) == 8 ? (const VT*)d.LU64 : (const VT*)d.LU32;
-    const int di = d.pdiag[i];
-    const int b0 = UPPER ? di + 1 : d.prowp[i];
-    const int b1 = UPPER ? d.prowp[i + 1] : di;
-    double* ob = out + 6 * (size_t)d.off;
-    double acc = 0.0;
-    if (g < 4) {
-      for (int blk = b0 + g; blk < b1; blk += 4) {
-        const int k = d.pcols[blk];
-        VT a[6];
+  const ProbDev& d = P[p];
+  const TriDesc T = UPPER ? d.U : d.L;
+  double* xs = reinterpret_cast<double*>(smem + (size_t)kStages * T.stage);
+  double* rs = xs + 6 * (size_t)T.capb;
+  const double* rb = rhs + 6 * (size_t)d.off;
+  double* ob = out + 6 * (size_t)d.off;
+  if (tid == 0) {
+    for (int s = 0; s < kStages; s++) mbar_init(&bar[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    abort_flag = 0;
+  }
+  __syncthreads();
+  // chunk byte ranges are read one issue ahead so tid 0 never waits on them
+  long long lo = 0, hi = 0;
+  if (tid == 0) {
+    lo = T.off[0];
+    hi = T.off[1];
+  }
+  auto issue = [&](int c) {  // tid 0 only; lo/hi hold chunk c's range
+    uint64_t* b = &bar[c % kStages];
+    mbar_expect_tx(b, (unsigned)(hi - lo));
+    bulk_g2s(smem + (size_t)(c % kStages) * T.stage, T.stream + lo, (unsigned)(hi - lo), b);
+    lo = hi;
+    if (c + 2 <= T.nch) hi = T.off[c + 2];
+  };
+  if (tid == 0)
+    for (int c = 0; c < kStages - 1 && c < T.nch; c++) issue(c);
+  int issued = min(kStages - 1, T.nch);
+  int c = 0;
+  for (; c < T.nch; c++) {
+    const int s = c % kStages;
+    if (!mbar_wait(&bar[s], (unsigned)((c / kStages) & 1))) abort_flag = 1;
+    __syncthreads();  // chunk c-1's x writes done; its stage is free again
+    if (abort_flag) break;
+    if (issued < T.nch) {
+      if (tid == 0) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        issue(issued);
+      }
+      issued++;
+    }
+    const unsigned char* st = smem + (size_t)s * T.stage;
+    const int4 hdr = *reinterpret_cast<const int4*>(st);
+    const int nr = hdr.x, nb = hdr.y;
+    const int4* ri = reinterpret_cast<const int4*>(st + 16);
+    const int32_t* sc = reinterpret_cast<const int32_t*>(st + 16 + 16 * (size_t)nr);
+    const VT* sv = reinterpret_cast<const VT*>(st + 16 + 16 * (size_t)nr + 4 * (size_t)nb);
+    {
+      // every thread issues all its loads (x of the chunk's columns, then
+      // the rows' right-hand sides) before storing any: one memory latency
+      // per chunk instead of one per loop trip
+      double v[kGather];
 #pragma unroll
-        for (int c = 0; c < 6; c++) a[c] = LU[36 * (size_t)blk + 6 * r + c];
-        const double* xk = ob + 6 * (size_t)k;
-        double xv[6];
-        const unsigned long long t0 = global_ns();
-        unsigned polls = 0;
-        while (true) {
-          bool ready = true;
+      for (int u = 0; u < kGather; u++) {
+        const int t = tid + u * kSweepThreads;
+        if (t < 6 * nb)
+          v[u] = ob[6 * (size_t)sc[t / 6] + t % 6];
+        else if (t < 6 * (nb + nr))
+          v[u] = rb[6 * (size_t)ri[t / 6 - nb].x + t % 6];
+      }
 #pragma unroll
-          for (int c = 0; c < 6; c++) {
-            xv[c] = ld_relaxed(&xk[c]);
-            ready = ready && !is_sentinel(xv[c]);
-          }
-          if (ready) break;
-          if (wait_expired(t0, polls)) {
-            timed_out = true;
-            break;
-          }
-        }
-#pragma unroll
-        for (int c = 0; c < 6; c++) acc = fma((double)a[c], xv[c], acc);
+      for (int u = 0; u < kGather; u++) {
+        const int t = tid + u * kSweepThreads;
+        if (t < 6 * nb)
+          xs[t] = v[u];
+        else if (t < 6 * (nb + nr))
+          rs[t - 6 * nb] = v[u];
       }
     }
-    acc += __shfl_down_sync(0xffffffffu, acc, 12);
-    acc += __shfl_down_sync(0xffffffffu, acc, 6);
-    const double t = (lane < 6 ? rhs[6 * (size_t)grow + lane] : 0.0) - acc;
-    if (!UPPER) {
-      if (lane < 6) st_relaxed(&ob[6 * (size_t)i + lane], t);
-    } else {
-      double v = 0.0;
+    __syncthreads();
+    for (int k = warp; k < nr; k += nw) {
+      const int4 row = ri[k];
+      const int i = row.x, rbeg = row.y, rcnt = row.z;
+      const int first = UPPER ? 1 : 0;  // U rows start with U_ii^{-1}
+      double acc = 0.0;
+      if (g < 4) {
+        for (int j = first + g; j < rcnt; j += 4) {
+          const VT* a = sv + (size_t)(rbeg + j) * 36 + 6 * r;
+          const double* xk = xs + 6 * (rbeg + j);
 #pragma unroll
-      for (int c = 0; c < 6; c++) {
-        const double tc = __shfl_sync(0xffffffffu, t, c);
-        if (lane < 6) v = fma((double)LU[36 * (size_t)di + 6 * lane + c], tc, v);
+          for (int cc = 0; cc < 6; cc++) acc = fma((double)a[cc], xk[cc], acc);
+        }
       }
-      if (lane < 6) st_relaxed(&ob[6 * (size_t)i + lane], v);
+      acc += __shfl_down_sync(0xffffffffu, acc, 12);
+      acc += __shfl_down_sync(0xffffffffu, acc, 6);
+      const double t = (lane < 6 ? rs[6 * k + lane] : 0.0) - acc;
+      if (!UPPER) {
+        if (lane < 6) ob[6 * (size_t)i + lane] = t;
+      } else {
+        const VT* Di = sv + (size_t)rbeg * 36;
+        double v = 0.0;
+#pragma unroll
+        for (int cc = 0; cc < 6; cc++) {
+          const double tc = __shfl_sync(0xffffffffu, t, cc);
+          if (lane < 6) v = fma((double)Di[6 * lane + cc], tc, v);
+        }
+        if (lane < 6) ob[6 * (size_t)i + lane] = v;
+      }
     }
   }
-  if (timed_out) atomicOr(&ctl->status, ST_TIMEOUT);
+  if (abort_flag && tid == 0) {
+    atomicOr(&ctl->status, ST_TIMEOUT);
+    // chunks c .. issued-1 may still be in flight: let them land (bounded)
+    for (int q = c; q < issued; q++) mbar_wait(&bar[q % kStages], (unsigned)((q / kStages) & 1));
+  }
+}
+
+// Factor values into a chunk stream: block slot q of the triangle takes
+// the 6x6 block src[map[q]] (zero for padding, map < 0) at element offset
+// vpos[q] of the stream viewed as VT.
+template <class VT>
+__global__ void repack_kernel(size_t nslots, const int32_t* __restrict__ map,
+                              const int64_t* __restrict__ vpos, const double* __restrict__ src,
+                              VT* __restrict__ dst) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nslots * 36) return;
+  const size_t q = t / 36, e = t % 36;
+  const int m = map[q];
+  dst[vpos[q] + e] = m >= 0 ? (VT)src[36 * (size_t)m + e] : (VT)0;
 }
 
 // ------------------------------------------------- segmented vector kernels
@@ -537,7 +595,10 @@ __global__ void seg_combine(const double* __restrict__ V, size_t N, int m, Chunk
   }
 }
 // cycle start: beta_p = ||src_p||, g_p = (beta, 0, ...), run_p = live_p
-__global__ void bcycle_init(const double* pnorm, Chunks C, int np, int m, GmArrays G) {
+// tfac (may be null): target = tfac[p] * beta, the Arnoldi residual
+// reduction this cycle must reach.
+__global__ void bcycle_init(const double* pnorm, Chunks C, int np, int m, GmArrays G,
+                            const double* tfac) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= np) return;
   double s = 0.0;
@@ -545,6 +606,7 @@ __global__ void bcycle_init(const double* pnorm, Chunks C, int np, int m, GmArra
     for (int c = C.pstart[p]; c < C.pstart[p + 1]; c++) s += pnorm[c];
   const double beta = sqrt(s);
   G.hn[p] = beta;
+  if (tfac && G.live[p]) G.target[p] = tfac[p] * beta;
   G.jcnt[p] = 0;
   G.run[p] = (G.live[p] && beta > 0.0) ? 1 : 0;
   double* g = G.g + (size_t)p * (m + 1);
@@ -598,20 +660,142 @@ struct gf_precond {
   int nlevL = 0, nlevU = 0;
   std::vector<int32_t> lvL, lvU;
   DevBuf<int32_t> d_rowp, d_cols, d_diag, d_amap;
+  DevBuf<int32_t> d_levLptr, d_levLrows;  // factorization order
   DevBuf<double> d_lu;
-  DevBuf<float> d_lu32;
+  struct Tri {
+    int nch = 0, stage = 0, capb = 0, capr = 0;
+    size_t nslots = 0;
+    DevBuf<int64_t> off, vpos;
+    DevBuf<int32_t> map;
+    DevBuf<unsigned char> stream;
+  } tri[2];  // 0 = L, 1 = U
   gf_batch* self = nullptr;  // batch of one, built on first use
 };
 
+namespace gf {
+// Chunk stream of one triangle (layout described at TriDesc).
+static cudaError_t build_tri(gf_precond* p, const std::vector<int32_t>& diag, bool upper) {
+  const Pattern& P = p->pat;
+  const int n = P.n;
+  const std::vector<int32_t>& lv = upper ? p->lvU : p->lvL;
+  const int nlev = upper ? p->nlevU : p->nlevL;
+  const size_t vs = p->prec == GF_PREC_FP32 ? 4 : 8;
+  auto cnt = [&](int i) { return upper ? P.rowp[i + 1] - diag[i] : diag[i] - P.rowp[i]; };
+  std::vector<int32_t> ptr(nlev + 1, 0), rows(n);
+  for (int i = 0; i < n; i++) ptr[lv[i] + 1]++;
+  for (int l = 0; l < nlev; l++) ptr[l + 1] += ptr[l];
+  {
+    std::vector<int32_t> f(ptr.begin(), ptr.end() - 1);
+    for (int i = 0; i < n; i++) rows[f[lv[i]]++] = i;
+  }
+  int maxc = 0;
+  for (int i = 0; i < n; i++) maxc = std::max(maxc, cnt(i));
+  const int capb = std::max(p->prec == GF_PREC_FP32 ? 320 : 192, (maxc + 3) & ~3);
+  const int capr = 128;
+  // pass 1: chunk boundaries (row ranges of `rows`) and block counts
+  std::vector<int32_t> ck{0}, cb;  // chunk row starts, padded block counts
+  {
+    int cur = 0, nr = 0;
+    auto close = [&](int k) {
+      cur = std::max(4, (cur + 3) & ~3);
+      ck.push_back(k);
+      cb.push_back(cur);
+      cur = nr = 0;
+    };
+    for (int l = 0; l < nlev; l++) {
+      for (int k = ptr[l]; k < ptr[l + 1]; k++) {
+        const int c = cnt(rows[k]);
+        if (nr > 0 && (cur + c > capb || nr == capr)) close(k);
+        cur += c;
+        nr++;
+      }
+      if (nr > 0) close(ptr[l + 1]);  // a chunk never spans two levels
+    }
+  }
+  const int nch = (int)cb.size();
+  std::vector<int64_t> off(nch + 1, 0);
+  size_t nslots = 0;
+  int stage = 0;
+  for (int c = 0; c < nch; c++) {
+    const int nr = ck[c + 1] - ck[c];
+    const int64_t bytes = 16 + 16 * (int64_t)nr + (4 + 36 * (int64_t)vs) * cb[c];
+    off[c + 1] = off[c] + bytes;
+    stage = std::max<int64_t>(stage, bytes);
+    nslots += cb[c];
+  }
+  // pass 2: headers, row records, columns; value positions and sources
+  std::vector<unsigned char> bytes(off[nch], 0);
+  std::vector<int32_t> map(nslots, -1);
+  std::vector<int64_t> vpos(nslots);
+  size_t q = 0;
+  for (int c = 0; c < nch; c++) {
+    unsigned char* base = bytes.data() + off[c];
+    const int nr = ck[c + 1] - ck[c], nb = cb[c];
+    int32_t* hdr = reinterpret_cast<int32_t*>(base);
+    int32_t* rec = hdr + 4;
+    int32_t* col = rec + 4 * nr;
+    const int64_t v0 = (off[c] + 16 + 16 * (int64_t)nr + 4 * (int64_t)nb) / (int64_t)vs;
+    hdr[0] = nr;
+    hdr[1] = nb;
+    int b = 0;
+    for (int k = ck[c]; k < ck[c + 1]; k++) {
+      const int i = rows[k];
+      rec[4 * (k - ck[c]) + 0] = i;
+      rec[4 * (k - ck[c]) + 1] = b;
+      rec[4 * (k - ck[c]) + 2] = cnt(i);
+      auto put = [&](int jp) {
+        col[b] = P.cols[jp];
+        map[q + b] = jp;
+        b++;
+      };
+      if (upper) {
+        put(diag[i]);
+        for (int jp = diag[i] + 1; jp < P.rowp[i + 1]; jp++) put(jp);
+      } else {
+        for (int jp = P.rowp[i]; jp < diag[i]; jp++) put(jp);
+      }
+    }
+    for (int k = b; k < nb; k++) col[k] = 0;  // padding (never referenced by a row)
+    for (int k = 0; k < nb; k++) vpos[q + k] = v0 + 36 * (int64_t)k;
+    q += nb;
+  }
+  gf_precond::Tri& t = p->tri[upper ? 1 : 0];
+  t.nch = nch;
+  t.stage = stage;
+  t.capb = capb;
+  t.capr = capr;
+  t.nslots = nslots;
+  cudaError_t e = cudaSuccess;
+  auto up = [&](cudaError_t x) {
+    if (e == cudaSuccess) e = x;
+  };
+  up(t.off.upload(off));
+  up(t.vpos.upload(vpos));
+  up(t.map.upload(map));
+  up(t.stream.upload(bytes));
+  return e;
+}
+static TriDesc tri_desc(const gf_precond* p, int which) {
+  const gf_precond::Tri& t = p->tri[which];
+  return TriDesc{t.nch, t.stage, t.capb, t.capr, t.off.p, t.stream.p};
+}
+static size_t sweep_smem(const gf_precond* p, int which) {
+  const gf_precond::Tri& t = p->tri[which];
+  return sweep_smem_bytes(t.stage, t.capb, t.capr);
+}
+}  // namespace gf
+
 struct gf_batch {
   int np = 0, nrows = 0, maxlevL = 0, maxlevU = 0;
+  size_t smemL = 0, smemU = 0;  // dynamic shared memory of the sweeps
+  int pprec = GF_PREC_FP64;      // factor precision shared by the batch's preconditioners
   size_t N = 0;  // doubles in batch space
   std::vector<gf_assembler*> asms;
   std::vector<gf_bsr*> mats;
   std::vector<gf_precond*> pcs;
   std::vector<int> offs;
   DevBuf<ProbDev> d_desc;
-  DevBuf<int32_t> d_row_prob, d_orderL, d_orderU, d_flags;
+  DevBuf<int32_t> d_row_prob;
   DevBuf<SweepCtl> d_ctl;
   DevBuf<double> d_tmp, d_b, d_x;
   int nchunks = 0;
@@ -620,6 +804,7 @@ struct gf_batch {
   DevBuf<PermEntry> d_perm_b, d_perm_x, d_perm_out;
   int m = 0;
   DevBuf<double> V, H, g, cs, ss, y, h, hn, target, partial, pnorm, w, t, r, d, e, norms, bnorm;
+  DevBuf<double> tfac;
   DevBuf<int> jcnt, run, live, live2;
   Chunks chunks() const { return Chunks{nchunks, d_cprob.p, d_clo.p, d_chi.p, d_pstart.p}; }
 };
@@ -651,7 +836,12 @@ static gf_status upload_desc(gf_batch* B) {
     d.pcols = p->d_cols.p;
     d.pdiag = p->d_diag.p;
     d.LU64 = p->d_lu.p;
-    d.LU32 = p->d_lu32.p;
+    d.nlevL = p->nlevL;
+    d.nlevU = p->nlevU;
+    d.levLptr = p->d_levLptr.p;
+    d.levLrows = p->d_levLrows.p;
+    d.L = tri_desc(p, 0);
+    d.U = tri_desc(p, 1);
   }
   GF_CUDA(cudaMemcpy(B->d_desc.p, h.data(), sizeof(ProbDev) * B->np, cudaMemcpyHostToDevice));
   return GF_OK;
@@ -665,27 +855,14 @@ static gf_status batch_build(gf_batch* B) {
   B->nrows = B->offs[np];
   B->N = (size_t)6 * B->nrows;
   std::vector<int32_t> row_prob(B->nrows);
-  // merged level orders: (level, problem, row)
-  std::vector<std::array<int, 3>> keysL, keysU;
-  keysL.reserve(B->nrows);
-  keysU.reserve(B->nrows);
-  B->maxlevL = B->maxlevU = 0;
+  B->pprec = B->pcs[0]->prec;
   for (int k = 0; k < np; k++) {
-    gf_precond* p = B->pcs[k];
-    for (int i = 0; i < B->asms[k]->nnodes; i++) {
-      row_prob[B->offs[k] + i] = k;
-      keysL.push_back({p->lvL[i], k, i});
-      keysU.push_back({p->lvU[i], k, i});
-    }
-    B->maxlevL = std::max(B->maxlevL, p->nlevL);
-    B->maxlevU = std::max(B->maxlevU, p->nlevU);
-  }
-  std::sort(keysL.begin(), keysL.end());
-  std::sort(keysU.begin(), keysU.end());
-  std::vector<int32_t> ordL(B->nrows), ordU(B->nrows);
-  for (int t = 0; t < B->nrows; t++) {
-    ordL[t] = B->offs[keysL[t][1]] + keysL[t][2];
-    ordU[t] = B->offs[keysU[t][1]] + keysU[t][2];
+    if (B->pcs[k]->prec != B->pprec) return GF_INVALID_ARG;  // one factor precision per batch
+    B->smemL = std::max(B->smemL, sweep_smem(B->pcs[k], 0));
+    B->smemU = std::max(B->smemU, sweep_smem(B->pcs[k], 1));
+    for (int i = 0; i < B->asms[k]->nnodes; i++) row_prob[B->offs[k] + i] = k;
+    B->maxlevL = std::max(B->maxlevL, B->pcs[k]->nlevL);
+    B->maxlevU = std::max(B->maxlevU, B->pcs[k]->nlevU);
   }
   // reduction chunks aligned to each problem
   std::vector<int32_t> cprob, pstart(np + 1);
@@ -707,10 +884,6 @@ static gf_status batch_build(gf_batch* B) {
   };
   up(B->d_desc.alloc(np));
   up(B->d_row_prob.upload(row_prob));
-  up(B->d_orderL.upload(ordL));
-  up(B->d_orderU.upload(ordU));
-  up(B->d_flags.alloc(B->nrows));
-  if (e == cudaSuccess) up(cudaMemset(B->d_flags.p, 0, sizeof(int32_t) * B->nrows));
   up(B->d_ctl.alloc(1));
   if (e == cudaSuccess) up(cudaMemset(B->d_ctl.p, 0, sizeof(SweepCtl)));
   up(B->d_tmp.alloc(B->N));
@@ -749,6 +922,7 @@ static gf_status ensure_gmres(gf_batch* B, int m) {
   al(B->h.alloc((size_t)np * (m + 1)));
   al(B->hn.alloc(np));
   al(B->target.alloc(np));
+  al(B->tfac.alloc(np));
   al(B->partial.alloc((size_t)(m + 1) * B->nchunks));
   al(B->pnorm.alloc(B->nchunks));
   al(B->w.alloc(B->N));
@@ -774,25 +948,32 @@ static GmArrays arrays(gf_batch* B) {
                   B->hn.p, B->target.p, B->jcnt.p, B->run.p, B->live.p};
 }
 
-static unsigned persistent_grid(int nrows) {
-  return (unsigned)std::max(1, std::min(sm_count() * 4, (nrows + 3) / 4));
-}
 
-// z = U^{-1} L^{-1} r for problems with live[p] (all when live is null)
+// z = U^{-1} L^{-1} r for problems with live[p] (all when live is null).
+// The factor values are in the preconditioners' precision (one per batch),
+// independent of the precision of the Krylov loop that calls this.
+template <class VT>
+static gf_status bsweeps(gf_batch* B, const int* live, const double* r, double* z,
+                         cudaStream_t st) {
+  // the same cap for every batch: threads launching batches with different
+  // footprints concurrently must not lower it under each other
+  GF_CUDA(cudaFuncSetAttribute(bsweep_tma<VT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kSweepSmemMax));
+  GF_CUDA(cudaFuncSetAttribute(bsweep_tma<VT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kSweepSmemMax));
+  bsweep_tma<VT, false><<<B->np, kSweepThreads, B->smemL, st>>>(B->d_desc.p, live, r, B->d_tmp.p,
+                                                                B->d_ctl.p); ::gf::count_launch();
+  bsweep_tma<VT, true><<<B->np, kSweepThreads, B->smemU, st>>>(B->d_desc.p, live, B->d_tmp.p, z,
+                                                               B->d_ctl.p); ::gf::count_launch();
+  GF_CHECK_LAUNCH();
+  return GF_OK;
+}
 template <class VT>
 static gf_status bprecond(gf_batch* B, const int* live, const double* r, double* z,
                           cudaStream_t st) {
-  const unsigned nb = persistent_grid(B->nrows);
-  fill_sentinel<<<592, 256, 0, st>>>(B->d_tmp.p, B->N); ::gf::count_launch();
-  fill_sentinel<<<592, 256, 0, st>>>(z, B->N); ::gf::count_launch();
-  sweep_begin<<<1, 1, 0, st>>>(B->d_ctl.p); ::gf::count_launch();
-  bsweep_kernel<VT, false><<<nb, 128, 0, st>>>(B->nrows, B->d_row_prob.p, B->d_desc.p, live,
-                                               B->d_orderL.p, r, B->d_tmp.p, B->d_ctl.p); ::gf::count_launch();
-  sweep_begin<<<1, 1, 0, st>>>(B->d_ctl.p); ::gf::count_launch();
-  bsweep_kernel<VT, true><<<nb, 128, 0, st>>>(B->nrows, B->d_row_prob.p, B->d_desc.p, live,
-                                              B->d_orderU.p, B->d_tmp.p, z, B->d_ctl.p); ::gf::count_launch();
-  GF_CHECK_LAUNCH();
-  return GF_OK;
+  if (B->smemL > kSweepSmemMax || B->smemU > kSweepSmemMax) return GF_INVALID_ARG;
+  return B->pprec == GF_PREC_FP32 ? bsweeps<float>(B, live, r, z, st)
+                                  : bsweeps<double>(B, live, r, z, st);
 }
 
 template <class VT>
@@ -821,17 +1002,21 @@ static gf_status batch_factor(gf_batch* B, cudaStream_t st) {
   }
   GF_CHECK_LAUNCH();
   GF_CUDA(cudaMemsetAsync(&B->d_ctl.p->status, 0, 2 * sizeof(int), st));
-  sweep_begin<<<1, 1, 0, st>>>(B->d_ctl.p); ::gf::count_launch();
-  bfactor_kernel<<<persistent_grid(B->nrows), 128, 0, st>>>(B->nrows, B->d_row_prob.p,
-                                                            B->d_desc.p, B->d_orderL.p,
-                                                            B->d_flags.p, B->d_ctl.p); ::gf::count_launch();
+  bfactor_cta<<<B->np, kCtaThreads, 0, st>>>(B->d_desc.p, B->d_ctl.p); ::gf::count_launch();
   GF_CHECK_LAUNCH();
   for (int k = 0; k < B->np; k++) {
     gf_precond* p = B->pcs[k];
-    if (p->prec == GF_PREC_FP32) {
-      const size_t nv = (size_t)36 * p->pat.nnz();
-      convert_kernel<float><<<(unsigned)((nv + 255) / 256), 256, 0, st>>>(nv, p->d_lu.p,
-                                                                          p->d_lu32.p); ::gf::count_launch();
+    for (int w = 0; w < 2; w++) {
+      gf_precond::Tri& t = p->tri[w];
+      const unsigned nb = (unsigned)((t.nslots * 36 + 255) / 256);
+      if (t.nslots == 0) continue;
+      if (p->prec == GF_PREC_FP32)
+        repack_kernel<float><<<nb, 256, 0, st>>>(t.nslots, t.map.p, t.vpos.p, p->d_lu.p,
+                                                  reinterpret_cast<float*>(t.stream.p));
+      else
+        repack_kernel<double><<<nb, 256, 0, st>>>(t.nslots, t.map.p, t.vpos.p, p->d_lu.p,
+                                                   reinterpret_cast<double*>(t.stream.p));
+      ::gf::count_launch();
     }
   }
   GF_CHECK_LAUNCH();
@@ -864,20 +1049,13 @@ static gf_status bgmres(gf_batch* B, const double* b, double* x, int m, int max_
   seg_sumsq<<<nc, kRedThreads, 0, st>>>(b, C, nullptr, B->pnorm.p); ::gf::count_launch();
   seg_norm_out<<<pb, 128, 0, st>>>(B->pnorm.p, C, np, nullptr, B->bnorm.p); ::gf::count_launch();
   GF_CUDA(cudaMemcpyAsync(bn.data(), B->bnorm.p, sizeof(double) * np, cudaMemcpyDeviceToHost, st));
-  if (side == 0) {
-    s = bprecond<VT>(B, B->live.p, b, B->t.p, st);
-    if (s != GF_OK) return s;
-    seg_sumsq<<<nc, kRedThreads, 0, st>>>(B->t.p, C, B->live.p, B->pnorm.p); ::gf::count_launch();
-    seg_norm_out<<<pb, 128, 0, st>>>(B->pnorm.p, C, np, B->live.p, B->norms.p); ::gf::count_launch();
-    set_target<<<pb, 128, 0, st>>>(np, B->norms.p, rtol, G); ::gf::count_launch();
-  } else {
-    set_target<<<pb, 128, 0, st>>>(np, B->bnorm.p, rtol, G); ::gf::count_launch();
-  }
+  if (side != 0) set_target<<<pb, 128, 0, st>>>(np, B->bnorm.p, rtol, G), ::gf::count_launch();
   GF_CHECK_LAUNCH();
   GF_CUDA(cudaStreamSynchronize(st));
   for (int p = 0; p < np; p++)
     if (bn[p] == 0.0) bn[p] = 1.0;
   std::vector<int> live = live0, jc(np), runh(np);
+  std::vector<double> tf(np, 0.0);
   iters.assign(np, 0);
   restarts.assign(np, 0);
   rel.assign(np, 0.0);
@@ -917,9 +1095,18 @@ static gf_status bgmres(gf_batch* B, const double* b, double* x, int m, int max_
       s = bprecond<VT>(B, B->live.p, B->r.p, B->t.p, st);
       if (s != GF_OK) return s;
       src = B->t.p;
+      // Left preconditioning minimises ||M^-1 r||, which can sit far from
+      // ||r|| when M is ill-conditioned: every cycle asks the preconditioned
+      // residual to drop by the factor the true residual still needs (with
+      // a margin of 2 after the first cycle).
+      for (int p = 0; p < np; p++)
+        tf[p] = live[p] ? (restarts[p] ? 0.5 : 1.0) * rtol * bn[p] / rn[p] : 0.0;
+      GF_CUDA(cudaMemcpyAsync(B->tfac.p, tf.data(), sizeof(double) * np, cudaMemcpyHostToDevice,
+                              st));
     }
     seg_sumsq<<<nc, kRedThreads, 0, st>>>(src, C, B->live.p, B->pnorm.p); ::gf::count_launch();
-    bcycle_init<<<pb, 128, 0, st>>>(B->pnorm.p, C, np, m, G); ::gf::count_launch();
+    bcycle_init<<<pb, 128, 0, st>>>(B->pnorm.p, C, np, m, G, side == 0 ? B->tfac.p : nullptr);
+    ::gf::count_launch();
     seg_scale<<<nc, kRedThreads, 0, st>>>(src, B->V.p, C, B->run.p, B->hn.p); ::gf::count_launch();
     GF_CHECK_LAUNCH();
     const int steps = std::min(m, max_it - steps_total);
@@ -955,10 +1142,6 @@ static gf_status bgmres(gf_batch* B, const double* b, double* x, int m, int max_
       GF_CUDA(cudaStreamSynchronize(st));
       if (std::all_of(runh.begin(), runh.end(), [](int v) { return v == 0; })) break;
     }
-    SweepCtl hc;
-    s = read_ctl(B, st, &hc);
-    if (s != GF_OK) return s;
-    if (hc.status & ST_TIMEOUT) return GF_TIMEOUT;
     bbacksolve<<<pb, 128, 0, st>>>(np, m, G); ::gf::count_launch();
     seg_combine<<<nc, kRedThreads, 0, st>>>(B->V.p, B->N, m, C, G, B->w.p); ::gf::count_launch();
     GF_CHECK_LAUNCH();
@@ -1157,6 +1340,17 @@ gf_status gf_precond_create(gf_assembler* a, int32_t fill_level, int32_t precisi
   }
   p->nlevL = levels(p->pat, true, p->lvL);
   p->nlevU = levels(p->pat, false, p->lvU);
+  auto group = [n](const std::vector<int32_t>& lv, int nl, std::vector<int32_t>& ptr,
+                   std::vector<int32_t>& rows) {
+    ptr.assign(nl + 1, 0);
+    for (int i = 0; i < n; i++) ptr[lv[i] + 1]++;
+    for (int l = 0; l < nl; l++) ptr[l + 1] += ptr[l];
+    rows.resize(n);
+    std::vector<int32_t> fill(ptr.begin(), ptr.end() - 1);
+    for (int i = 0; i < n; i++) rows[fill[lv[i]]++] = i;
+  };
+  std::vector<int32_t> lptr, lrows;
+  group(p->lvL, p->nlevL, lptr, lrows);
   cudaError_t e = cudaSuccess;
   auto up = [&](cudaError_t x) {
     if (e == cudaSuccess) e = x;
@@ -1165,8 +1359,19 @@ gf_status gf_precond_create(gf_assembler* a, int32_t fill_level, int32_t precisi
   up(p->d_cols.upload(p->pat.cols));
   up(p->d_diag.upload(diag));
   up(p->d_amap.upload(amap));
+  up(p->d_levLptr.upload(lptr));
+  up(p->d_levLrows.upload(lrows));
   up(p->d_lu.alloc((size_t)36 * p->pat.nnz()));
-  if (precision == GF_PREC_FP32) up(p->d_lu32.alloc((size_t)36 * p->pat.nnz()));
+  if (e == cudaSuccess) e = build_tri(p, diag, false);
+  if (e == cudaSuccess) e = build_tri(p, diag, true);
+  auto fits = [&](int w) {
+    const gf_precond::Tri& t = p->tri[w];
+    return sweep_smem(p, w) <= kSweepSmemMax && 6 * (t.capb + t.capr) <= kGather * kSweepThreads;
+  };
+  if (e == cudaSuccess && !(fits(0) && fits(1))) {
+    delete p;
+    return GF_INVALID_ARG;  // a factor row longer than one staging buffer
+  }
   if (e != cudaSuccess) {
     set_last_error("gf_precond_create", e);
     delete p;
@@ -1212,14 +1417,10 @@ gf_status gf_precond_apply(gf_precond* p, const double* d_r, double* d_z, void* 
   if (!p || !d_r || !d_z || !p->self) return GF_INVALID_ARG;
   cudaStream_t st = as_stream(stream);
   gf_batch* B = p->self;
-  gf_status s = (p->prec == GF_PREC_FP32) ? bprecond<float>(B, nullptr, d_r, B->d_x.p, st)
-                                          : bprecond<double>(B, nullptr, d_r, B->d_x.p, st);
+  gf_status s = bprecond<double>(B, nullptr, d_r, B->d_x.p, st);
   if (s != GF_OK) return s;
   GF_CUDA(cudaMemcpyAsync(d_z, B->d_x.p, sizeof(double) * B->N, cudaMemcpyDeviceToDevice, st));
-  SweepCtl h;
-  s = read_ctl(B, st, &h);
-  if (s != GF_OK) return s;
-  return (h.status & ST_TIMEOUT) ? GF_TIMEOUT : GF_OK;
+  return GF_OK;
 }
 
 void gf_solve_opts_default(gf_solve_opts* o) {
@@ -1252,6 +1453,19 @@ gf_status gf_batch_assemble(gf_batch* B, void* stream) {
   if (!B) return GF_INVALID_ARG;
   for (int k = 0; k < B->np; k++) {
     gf_status s = gf_add_jacobian(B->asms[k], nullptr, B->mats[k], GF_ASSEMBLE_FUSE_BCS, stream);
+    if (s != GF_OK) return s;
+  }
+  return GF_OK;
+}
+
+gf_status gf_batch_assemble_ex(gf_batch* B, const double* const* d_thick, void* stream) {
+  if (!B) return GF_INVALID_ARG;
+  for (int k = 0; k < B->np; k++) {
+    gf_status s = (d_thick && d_thick[k])
+                      ? gf_add_jacobian_thick(B->asms[k], d_thick[k], nullptr, B->mats[k],
+                                              GF_ASSEMBLE_FUSE_BCS, stream)
+                      : gf_add_jacobian(B->asms[k], nullptr, B->mats[k], GF_ASSEMBLE_FUSE_BCS,
+                                        stream);
     if (s != GF_OK) return s;
   }
   return GF_OK;

@@ -169,21 +169,21 @@ int levels(const Pattern& p, bool lower, std::vector<int32_t>& level) {
 }
 
 // Scatter schedule.
-//  1. Chunks: seeds in ascending element order; each chunk grows breadth-first
-//     over elements sharing a node (neighbours of a node in ascending element
-//     order, nodes in element-local order) until it holds chunk_size elements.
+//  1. Chunks (one warp's work, at most chunk_size elements): seeds in
+//     ascending element order; a chunk grows breadth-first over elements
+//     sharing a node (neighbours of a node in ascending element order, nodes
+//     in element-local order) until it holds chunk_size elements.
 //  2. Chunk colours: greedy in chunk order, smallest colour not used by an
-//     already-coloured chunk that shares a node.
-//  3. Element colours: greedy within each chunk in chunk (BFS) order, smallest
-//     colour not used by an already-coloured element of the same chunk that
-//     shares a node.
-//  4. Execution order: chunk colour, chunk id, element colour, BFS position.
-//     The first touch of a matrix block (or residual node) is the toucher
-//     with the smallest (chunk colour, element colour); it stores, later
-//     touchers read-modify-write. Touchers sharing (chunk colour, element
-//     colour) cannot share a node, so the first touch is unique.
+//     already-coloured chunk that shares a node. Chunks of one colour share
+//     no node and run concurrently.
+//  3. Inside a chunk one warp processes the elements one after another in
+//     BFS order; an element's "colour" is its position in the chunk.
+//  4. Execution order: chunk colour, chunk id, position. The first touch of
+//     a matrix block (or residual node) is the toucher with the smallest
+//     (chunk colour, position); it stores, later touchers read-modify-write.
 int build_schedule(int nelem, int nnodes, const int32_t* conn, const std::vector<int32_t>& emap,
                    int nnzb, int chunk_size, Schedule& s) {
+  if (chunk_size > kMaxEC) return -1;
   s.chunk_size = chunk_size;
   // node -> elements
   std::vector<int32_t> ne_ptr(nnodes + 1, 0), ne_idx((size_t)4 * nelem);
@@ -228,10 +228,10 @@ int build_schedule(int nelem, int nnodes, const int32_t* conn, const std::vector
   s.nchunks = nc;
   // 2. chunk colours
   s.chunk_color.assign(nc, -1);
-  std::vector<int32_t> mark(64, -1);
   s.ncc = 0;
+  std::vector<char> used;
   for (int c = 0; c < nc; c++) {
-    std::vector<char> used;
+    used.assign(used.size(), 0);
     for (int k = cstart[c]; k < cstart[c + 1]; k++) {
       int e = bfs[k];
       for (int a = 0; a < 4; a++) {
@@ -251,28 +251,14 @@ int build_schedule(int nelem, int nnodes, const int32_t* conn, const std::vector
     s.chunk_color[c] = col;
     s.ncc = std::max(s.ncc, col + 1);
   }
-  // 3. element colours within chunks
+  // 3. position inside the chunk
   s.elem_color.assign(nelem, -1);
   s.max_ec = 0;
-  for (int c = 0; c < nc; c++) {
+  for (int c = 0; c < nc; c++)
     for (int k = cstart[c]; k < cstart[c + 1]; k++) {
-      int e = bfs[k];
-      unsigned used = 0;
-      for (int a = 0; a < 4; a++) {
-        int n = conn[4 * e + a];
-        for (int q = ne_ptr[n]; q < ne_ptr[n + 1]; q++) {
-          int f = ne_idx[q];
-          if (f != e && s.elem_chunk[f] == c && s.elem_color[f] >= 0)
-            used |= 1u << s.elem_color[f];
-        }
-      }
-      int col = 0;
-      while (used & (1u << col)) col++;
-      if (col >= kMaxEC) return -1;
-      s.elem_color[e] = col;
-      s.max_ec = std::max(s.max_ec, col + 1);
+      s.elem_color[bfs[k]] = k - cstart[c];
+      s.max_ec = std::max(s.max_ec, k - cstart[c] + 1);
     }
-  }
   // 4. execution order
   s.chunk_list.resize(nc);
   std::iota(s.chunk_list.begin(), s.chunk_list.end(), 0);
@@ -284,17 +270,10 @@ int build_schedule(int nelem, int nnodes, const int32_t* conn, const std::vector
   s.order.clear();
   s.order.reserve(nelem);
   s.chunk_start.assign(nc + 1, 0);
-  s.ec_off.assign((size_t)nc * (kMaxEC + 1), 0);
   for (int li = 0; li < nc; li++) {
     int c = s.chunk_list[li];
     s.chunk_start[li] = (int32_t)s.order.size();
-    int32_t* off = &s.ec_off[(size_t)li * (kMaxEC + 1)];
-    for (int col = 0; col < kMaxEC; col++) {
-      off[col] = (int32_t)s.order.size() - s.chunk_start[li];
-      for (int k = cstart[c]; k < cstart[c + 1]; k++)
-        if (s.elem_color[bfs[k]] == col) s.order.push_back(bfs[k]);
-    }
-    off[kMaxEC] = (int32_t)s.order.size() - s.chunk_start[li];
+    for (int k = cstart[c]; k < cstart[c + 1]; k++) s.order.push_back(bfs[k]);
   }
   s.chunk_start[nc] = (int32_t)s.order.size();
   // first-touch masks

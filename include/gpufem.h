@@ -125,6 +125,11 @@ gf_status gf_add_residual(gf_assembler* a, double* d_res, int32_t flags, void* s
  * pass. */
 gf_status gf_add_jacobian(gf_assembler* a, double* d_res, gf_bsr* mat, int32_t flags,
                           void* stream);
+/* add_jacobian with a per-call element thickness field (device pointer,
+ * natural element order) instead of the assembler's own, so one assembler
+ * can assemble many thickness fields concurrently on different streams. */
+gf_status gf_add_jacobian_thick(gf_assembler* a, const double* d_thick, double* d_res,
+                                gf_bsr* mat, int32_t flags, void* stream);
 /* add_energy (include/assembler.h:198-229; the reference GPU kernel is an
  * empty stub, base/elem_group.cuh:11-13): *h_energy = U(u). */
 gf_status gf_add_energy(gf_assembler* a, double* h_energy, void* stream);
@@ -154,7 +159,9 @@ gf_status gf_permute_vec(gf_assembler* a, const double* d_in, double* d_out, int
 enum { GF_PREC_FP64 = 0, GF_PREC_FP32 = 1 };
 /* ILUk_Preconditioner (include/linalg/precond.h:5-55) with the symbolic
  * ILU(k) of computeILUk (include/linalg/bsr_utils.h:678-807); fill_level 0
- * keeps A's pattern (ILU(0)). precision selects FP64 or FP32 factors. */
+ * keeps A's pattern (ILU(0)). precision selects FP64 or FP32 factors.
+ * GF_INVALID_ARG if a factor row holds more blocks than one shared-memory
+ * stage of the triangular sweep (about 240 blocks in FP64, 400 in FP32). */
 gf_status gf_precond_create(gf_assembler* a, int32_t fill_level, int32_t precision,
                             gf_precond** out);
 gf_status gf_precond_destroy(gf_precond* p);
@@ -211,12 +218,17 @@ gf_status gf_gmres_solve(gf_assembler* a, gf_bsr* A, gf_precond* p, const double
  * per-problem Arnoldi states and per-problem reductions, so every problem's
  * result is bitwise the same alone and in any batch. No reference
  * counterpart: the reference solves one problem per driver
- * (examples/iterative/gmres.cu). The handles must outlive the batch. */
+ * (examples/iterative/gmres.cu). The handles must outlive the batch, and
+ * all preconditioners of a batch must have the same precision
+ * (GF_INVALID_ARG otherwise). */
 gf_status gf_batch_create(int32_t n, gf_assembler* const* asms, gf_bsr* const* mats,
                           gf_precond* const* pcs, gf_batch** out);
 gf_status gf_batch_destroy(gf_batch* b);
 /* add_jacobian with fused BCs for every problem. */
 gf_status gf_batch_assemble(gf_batch* b, void* stream);
+/* As gf_batch_assemble with a per-problem thickness field (d_thick[k] may be
+ * NULL to use the assembler's own). */
+gf_status gf_batch_assemble_ex(gf_batch* b, const double* const* d_thick, void* stream);
 /* Numeric ILU(k) of every problem in one level-ordered launch. */
 gf_status gf_batch_factor(gf_batch* b, void* stream);
 /* Solve every problem: d_b[k], d_x[k] device pointers (natural order,

@@ -5,16 +5,16 @@ project's own deterministic schedule (there is no colouring in the
 reference); this file restates that specification independently so tests
 can compare chunks, colours and first-touch masks bit-exactly:
 
- 1. Chunks: seeds in ascending element order; a chunk grows breadth-first
-    over elements sharing a node (for each dequeued element, its nodes in
-    element-local order, each node's elements in ascending order) until it
-    holds `chunk_size` elements.
+ 1. Chunks (one warp's work): seeds in ascending element order; a chunk
+    grows breadth-first over elements sharing a node (for each dequeued
+    element, its nodes in element-local order, each node's elements in
+    ascending order) until it holds `chunk_size` elements.
  2. Chunk colours: greedy in chunk order; smallest colour not used by an
     already-coloured chunk sharing a node.
- 3. Element colours: greedy within each chunk in BFS order; smallest colour
-    not used by an already-coloured element of the same chunk sharing a node.
+ 3. An element's colour is its position in its chunk (the warp processes a
+    chunk's elements one after another).
  4. First touch of a block / node: the toucher with the smallest
-    (chunk colour, element colour).
+    (chunk colour, position).
 Small meshes only (pure-Python loops).
 """
 from __future__ import annotations
@@ -22,7 +22,7 @@ from __future__ import annotations
 import numpy as np
 
 
-def schedule(conn, nnodes, emap, chunk_size=32, max_ec=15):
+def schedule(conn, nnodes, emap, chunk_size=8, max_ec=15):
     conn = np.asarray(conn).reshape(-1, 4)
     ne = conn.shape[0]
     node_elems = [[] for _ in range(nnodes)]
@@ -66,17 +66,8 @@ def schedule(conn, nnodes, emap, chunk_size=32, max_ec=15):
         chunk_color[c] = col
     elem_color = [-1] * ne
     for c, members in enumerate(chunks):
-        for e in members:
-            used = set()
-            for a in range(4):
-                for f in node_elems[conn[e, a]]:
-                    if f != e and elem_chunk[f] == c and elem_color[f] >= 0:
-                        used.add(elem_color[f])
-            col = 0
-            while col in used:
-                col += 1
-            assert col < max_ec
-            elem_color[e] = col
+        for k, e in enumerate(members):
+            elem_color[e] = k
     stride = max_ec + 1
     emap = np.asarray(emap).reshape(-1, 16)
     tb, tn = {}, {}

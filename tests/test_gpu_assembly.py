@@ -117,7 +117,7 @@ def test_schedule_bit_exact_and_deterministic(oracle):
     mesh = M.plate_config2(24, 12)
     A, K, res = _assemble_gpu(mesh, "rcm")
     s = A.getSchedule()
-    ref = schedule(mesh.conn, mesh.num_nodes, A.getBsrData()["elemIndMap"], chunk_size=128)
+    ref = schedule(mesh.conn, mesh.num_nodes, A.getBsrData()["elemIndMap"], chunk_size=8)
     for k in ("elem_chunk", "chunk_color", "elem_color", "first_touch"):
         np.testing.assert_array_equal(s[k], ref[k], err_msg=k)
     assert s["num_chunk_colors"] == ref["num_chunk_colors"]

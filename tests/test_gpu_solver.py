@@ -60,34 +60,51 @@ def test_ilu_factor_and_apply_match_oracle(oracle, fill):
         vals_k = vals
     st, lu_ref = oracle.ilu0(r2, c2, vals_k)
     assert st == 0
-    # Off-diagonal blocks compare directly, diagonal blocks against the
-    # inverse (the GPU stores U_ii^{-1}). Block ILU on these shells is
-    # numerically unstable (factor growth ~1e13), so rounding-order
-    # differences between two correct factorizations grow along the
-    # elimination: 1e-8 normwise is the bar, and run-to-run equality is
-    # checked bitwise below.
+    # Block ILU on these shells is numerically unstable (factor growth
+    # ~1e13), so two correct factorizations that round in a different order
+    # differ entrywise far above machine precision. Parity is judged by what
+    # ILU(k) defines: (L U)_ij = A_ij on the pattern (backward error), for the
+    # GPU factors (diagonal blocks hold U_ii^{-1}) and for the oracle's, plus
+    # bitwise run-to-run equality.
     n = len(r2) - 1
-    G = lu_gpu.reshape(-1, 6, 6)
-    R = lu_ref.reshape(-1, 6, 6)
-    off = np.ones(len(c2), bool)
+    G = lu_gpu.reshape(-1, 6, 6).copy()
     for i in range(n):
         for jp in range(r2[i], r2[i + 1]):
             if c2[jp] == i:
-                off[jp] = False
-                Ri = np.linalg.inv(R[jp])
-                assert np.abs(G[jp] - Ri).max() <= 1e-6 * np.abs(Ri).max()
-    assert np.abs(G[off] - R[off]).max() <= 1e-8 * np.abs(R[off]).max()
+                G[jp] = np.linalg.inv(G[jp])
+    A_d = oracle.bsr_to_dense(r2, c2, vals_k)
+    mask = oracle.bsr_to_dense(r2, c2, np.ones(36 * len(c2))) != 0
+
+    def backward(F):
+        """max |(L U - A)_ij| over the pattern / max |A| for block factors F."""
+        N = 6 * n
+        Lm, Um = np.eye(N), np.zeros((N, N))
+        for i in range(n):
+            for jp in range(r2[i], r2[i + 1]):
+                j = c2[jp]
+                tgt = Lm if j < i else Um
+                tgt[6 * i:6 * i + 6, 6 * j:6 * j + 6] = F[jp]
+        LU = Lm @ Um
+        return np.abs((LU - A_d)[mask]).max() / np.abs(A_d).max(), Lm, Um
+
+    eg, Lg, Ug = backward(G)
+    eo, _, _ = backward(lu_ref.reshape(-1, 6, 6))
+    assert eo <= 1e-10, eo
+    assert eg <= 1e-10, eg
     P.factor(K)
     torch.cuda.synchronize()
     _, _, lu_again = P.get()
     assert np.array_equal(lu_again.view(np.uint64), lu_gpu.view(np.uint64))
+    # the apply solves L U z = r with the GPU factors (triangular solves are
+    # backward stable)
     r = np.random.default_rng(2).standard_normal(mesh.num_dof)
-    z_ref = oracle.ilu0_apply(r2, c2, lu_ref, r)
     rt = torch.tensor(r, device="cuda")
     zt = torch.zeros_like(rt)
     P.apply(rt, zt)
     z = zt.cpu().numpy()
-    assert np.abs(z - z_ref).max() <= 1e-6 * np.abs(z_ref).max()
+    res = Lg @ (Ug @ z) - r
+    scale = np.abs(Lg).max() * np.abs(Ug).max() * np.abs(z).max() * len(z)
+    assert np.abs(res).max() <= 1e-13 * scale
 
 
 @pytest.mark.parametrize("side", [0, 1])
@@ -118,8 +135,11 @@ def test_mixed_precision_refinement_reaches_fp64_tolerance(oracle):
                                  _to_solver(mesh.loads, perm))
     x_dense = x_dense.reshape(-1, 6)[perm].ravel()
     b = torch.tensor(mesh.loads, device="cuda")
+    # block ILU(k) convergence is not monotonic in k on thin shells: on this
+    # plate the oracle's own ILU(2) stalls in right-preconditioned GMRES(200)
+    # while ILU(1) and ILU(3) converge, so ILU(3) is used
     for mixed, prec in ((0, "fp64"), (1, "fp32")):
-        P = ILUk_Preconditioner(A, fill_level=2, precision=prec)
+        P = ILUk_Preconditioner(A, fill_level=3, precision=prec)
         P.factor(K)
         x = torch.zeros_like(b)
         st, stats = gmres_solve(A, K, P, b, x, SolveOptions(restart=200, max_iters=4000,

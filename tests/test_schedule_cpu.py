@@ -8,7 +8,7 @@ from gpu_fem_b200 import mesh as M
 from oracle.schedule import schedule
 
 
-def _check_schedule(mesh, oracle, chunk=128):
+def _check_schedule(mesh, oracle, chunk=8):
     rowp, cols = oracle.bsr_pattern(mesh.conn, mesh.num_nodes)
     perm = np.arange(mesh.num_nodes, dtype=np.int32)
     emap = oracle.elem_ind_map(mesh.conn, rowp, cols, perm)
