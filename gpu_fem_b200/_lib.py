@@ -92,6 +92,7 @@ SIGNATURES = {
     "gf_precond_destroy": (_I, [_P]),
     "gf_precond_factor": (_I, [_P, _P, _P]),
     "gf_precond_apply": (_I, [_P, _P, _P, _P]),
+    "gf_precond_apply_noalloc": (_I, [_P, _P, _P, _P]),
     "gf_precond_info": (_I, [_P, _PI, _PI, _PI]),
     "gf_precond_get": (_I, [_P, _PI, _PI, _PD]),
     "gf_solve_opts_default": (None, [C.POINTER(gf_solve_opts)]),

@@ -10,6 +10,7 @@ static thread_local std::string g_last_error;
 void set_last_error(const char* where, cudaError_t e) {
   g_last_error = std::string(where) + ": " + cudaGetErrorString(e);
 }
+void set_last_error_text(const std::string& text) { g_last_error = text; }
 static std::atomic<long long> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 }  // namespace gf

@@ -13,6 +13,7 @@ namespace gf {
 
 // Thread-local text of the last CUDA error seen by the library.
 void set_last_error(const char* where, cudaError_t e);
+void set_last_error_text(const std::string& text);
 // Process-wide count of kernels this library has launched.
 void count_launch();
 

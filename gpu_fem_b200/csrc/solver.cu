@@ -26,6 +26,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 
 #include "gf_internal.h"
@@ -1420,6 +1421,69 @@ gf_status gf_precond_apply(gf_precond* p, const double* d_r, double* d_z, void* 
   gf_status s = bprecond<double>(B, nullptr, d_r, B->d_x.p, st);
   if (s != GF_OK) return s;
   GF_CUDA(cudaMemcpyAsync(d_z, B->d_x.p, sizeof(double) * B->N, cudaMemcpyDeviceToDevice, st));
+  return GF_OK;
+}
+
+// ---- preconditioner apply without allocation --------------------------
+// The intermediate vector of gf_precond_apply_noalloc. One array per device
+// for the whole process; its address on a device is looked up once, by the
+// first call made with that device current.
+static __device__ __align__(256) double g_noalloc_y[GF_NOALLOC_MAX_DOUBLES];
+static constexpr int kNoAllocDevices = 64;
+static std::mutex g_noalloc_mu;
+static double* g_noalloc_ptr[kNoAllocDevices] = {};
+
+gf_status gf_precond_apply_noalloc(gf_precond* p, const double* d_r, double* d_z, void* stream) {
+  if (!p || !d_r || !d_z || !p->self) return GF_INVALID_ARG;
+  gf_batch* B = p->self;
+  const size_t need = (size_t)6 * p->pat.n;
+  if (need > (size_t)GF_NOALLOC_MAX_DOUBLES) {
+    set_last_error_text("gf_precond_apply_noalloc: the problem needs " + std::to_string(need) +
+                        " doubles of scratch, more than the fixed " +
+                        std::to_string(GF_NOALLOC_MAX_DOUBLES));
+    return GF_INVALID_ARG;
+  }
+  int dev = 0;
+  GF_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocDevices) return GF_INVALID_ARG;
+  double* y = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+      void* a = nullptr;
+      GF_CUDA(cudaGetSymbolAddress(&a, g_noalloc_y));
+      g_noalloc_ptr[dev] = static_cast<double*>(a);
+    }
+    y = g_noalloc_ptr[dev];
+  }
+  if (B->smemL > kSweepSmemMax || B->smemU > kSweepSmemMax) return GF_INVALID_ARG;
+  cudaStream_t st = as_stream(stream);
+  // the same two sweep kernels as gf_precond_apply; y in the fixed array and
+  // z written straight into d_z (a batch of one starts at offset 0)
+  if (p->prec == GF_PREC_FP32) {
+    GF_CUDA(cudaFuncSetAttribute(bsweep_tma<float, false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSweepSmemMax));
+    GF_CUDA(cudaFuncSetAttribute(bsweep_tma<float, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSweepSmemMax));
+    bsweep_tma<float, false><<<1, kSweepThreads, B->smemL, st>>>(B->d_desc.p, nullptr, d_r, y,
+                                                                 B->d_ctl.p);
+    ::gf::count_launch();
+    bsweep_tma<float, true><<<1, kSweepThreads, B->smemU, st>>>(B->d_desc.p, nullptr, y, d_z,
+                                                                B->d_ctl.p);
+    ::gf::count_launch();
+  } else {
+    GF_CUDA(cudaFuncSetAttribute(bsweep_tma<double, false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSweepSmemMax));
+    GF_CUDA(cudaFuncSetAttribute(bsweep_tma<double, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSweepSmemMax));
+    bsweep_tma<double, false><<<1, kSweepThreads, B->smemL, st>>>(B->d_desc.p, nullptr, d_r, y,
+                                                                  B->d_ctl.p);
+    ::gf::count_launch();
+    bsweep_tma<double, true><<<1, kSweepThreads, B->smemU, st>>>(B->d_desc.p, nullptr, y, d_z,
+                                                                 B->d_ctl.p);
+    ::gf::count_launch();
+  }
+  GF_CHECK_LAUNCH();
   return GF_OK;
 }
 

@@ -171,6 +171,23 @@ gf_status gf_precond_factor(gf_precond* p, gf_bsr* A, void* stream);
 /* z = U^{-1} L^{-1} r (two cusparseDbsrsv2_solve calls,
  * examples/iterative/gmres.cu:522-532), solver ordering. */
 gf_status gf_precond_apply(gf_precond* p, const double* d_r, double* d_z, void* stream);
+/* As gf_precond_apply, but the call allocates no device memory. No
+ * counterpart in the reference. For callers that must not allocate while
+ * they run: a serving loop that reserved its HBM up front, or host code
+ * whose streams must not be stalled by the device-wide synchronisation an
+ * allocation or free can cause.
+ * The intermediate vector y = L^{-1} r lives in one fixed device array of
+ * GF_NOALLOC_MAX_DOUBLES doubles (2 MiB) inside the library; problems with
+ * 6 * num_nodes above that return GF_INVALID_ARG (text in gf_last_error) and
+ * run nothing. No entry of the array needs to start at zero: the lower
+ * sweep writes every entry the upper sweep reads.
+ * The first call on a device (with that device current) looks up the
+ * array's address on that device; make that first call before any stream
+ * capture. All calls in the process share the one array per device, which
+ * keeps the last call's contents; calls whose work overlaps on the GPU
+ * (different streams, no ordering between them) race on it. */
+#define GF_NOALLOC_MAX_DOUBLES 262144
+gf_status gf_precond_apply_noalloc(gf_precond* p, const double* d_r, double* d_z, void* stream);
 /* Pattern, level count and factor copy for checking. rowPtr/colPtr may be
  * NULL; values receives nnzb_pc*36 entries with the diagonal blocks holding
  * U_ii^{-1}. */
