@@ -44,7 +44,32 @@ def _args():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--problems", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sweep-case", action="store_true",
+                    help="small profiling case: the triangular sweeps of one 256x128 plate, "
+                         "ILU(6), FP32 factors, applied 5 times (no JSON line)")
     return ap.parse_args()
+
+
+def sweep_case():
+    """One preconditioner (256x128 clamped plate, t = 2 mm, RCM, ILU(6), FP32
+    factors, ~150 MB of factor) applied 5 times: the small case on which the
+    sweep kernel is profiled."""
+    import torch
+    from gpu_fem_b200 import mesh as M
+    from gpu_fem_b200.assembler import ElementAssembler, ILUk_Preconditioner, createBsrMat
+    m = M.plate(256, 128, 1.0, 0.5, lambda x, y: 0.002 + 0 * x, "all_edges",
+                lambda q: 1e3 + 0 * q[:, 0])
+    A = ElementAssembler.from_mesh(m, ordering="rcm")
+    K = createBsrMat(A)
+    A.add_jacobian(None, K, fuse_bcs=True)
+    P = ILUk_Preconditioner(A, fill_level=6, precision="fp32")
+    P.factor(K)
+    r = torch.randn(m.num_dof, dtype=torch.float64, device="cuda")
+    z = torch.zeros_like(r)
+    for _ in range(5):
+        P.apply(r, z)
+    torch.cuda.synchronize()
+    print("sweep case", P.info(), float(z.abs().max()))
 
 
 def _peaks():
@@ -225,6 +250,8 @@ def _default_fill(mesh):
 
 def main():
     args = _args()
+    if args.sweep_case:
+        return sweep_case()
     if args.impl == "reference":
         return run_reference(args)
     import numpy as np
@@ -252,12 +279,16 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    def timed(mixed, host_io=None):
+    def timed(mixed, host_io=None, sweep_timing=False):
+        import ctypes as C
         for _ in range(args.warmup):
             bs.step(mixed, host_io)
         barrier()
+        if sweep_timing:
+            L.check(L.lib().gf_timing_enable(1), "timing")
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
         c0 = L.lib().gf_launch_count()
+        torch.cuda.nvtx.range_push("timed")
         ev[0].record()
         its = []
         for k in range(args.steps):
@@ -265,7 +296,13 @@ def main():
             ev[k + 1].record()
             its.append(max(s["iterations"] for s in stats))
         barrier()
+        torch.cuda.nvtx.range_pop()
         timed.launches = L.lib().gf_launch_count() - c0
+        if sweep_timing:
+            sm, sl, sb = C.c_double(), C.c_longlong(), C.c_double()
+            L.check(L.lib().gf_timing_read(C.byref(sm), C.byref(sl), C.byref(sb)), "timing")
+            L.check(L.lib().gf_timing_enable(0), "timing")
+            timed.sweep = (sm.value, sl.value, sb.value)
         lat = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
         ms = ev[0].elapsed_time(ev[-1]) / args.steps
         if ws > 1:
@@ -278,8 +315,9 @@ def main():
 
     clocks = ClockSampler(local)
     clocks.start()
-    ms_mixed, lat_mixed = timed(True)
+    ms_mixed, lat_mixed = timed(True, sweep_timing=True)
     launches = timed.launches
+    sweep_ms, sweep_launches, sweep_bytes = timed.sweep
     its_mixed = timed.iters
     clk = clocks.stop()
     ms_fp64, lat_fp64 = timed(False)
@@ -292,31 +330,12 @@ def main():
     nprob = len(meshes)
     value = ws * nprob / (ms_mixed / 1e3)
 
-    # roofline: block triangular solves (the dominant kernel) on the largest problem
-    ib = max(range(nprob), key=lambda i: meshes[i].num_nodes)
+    # roofline of the dominant kernel, the block triangular sweeps
+    # (bsweep_tma), from CUDA events around every sweep pair inside the timed
+    # mixed-precision region and the algorithmic bytes the sweeps report
     peak, peak_kind = _peaks()
-    from gpu_fem_b200.assembler import ILUk_Preconditioner
-    P = ILUk_Preconditioner(bs.asms[ib], bs.fills[ib], "fp32")
-    P.factor(bs.mats[ib])
-    inf = P.info()
-    r = torch.randn(meshes[ib].num_dof, dtype=torch.float64, device="cuda")
-    z = torch.zeros_like(r)
-    reps = 20
-    for _ in range(3):
-        P.apply(r, z)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(reps):
-        P.apply(r, z)
-    e1.record()
-    torch.cuda.synchronize()
-    ms_apply = e0.elapsed_time(e1) / reps
-    n = meshes[ib].num_nodes
-    # algorithmic bytes of L + U sweeps (FP32 values): values + column indices +
-    # row pointers twice + rhs/solution vectors twice (8-byte)
-    bytes_apply = inf["nnzb"] * (36 * 4 + 4) + 8 * (n + 1) + 6 * n * 2 * (8 + 8)
-    achieved = bytes_apply / (ms_apply / 1e3) / 1e9
+    sweep_s = sweep_ms / 1e3
+    achieved = sweep_bytes / sweep_s / 1e9 if sweep_s > 0 else 0.0
 
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws,
@@ -339,11 +358,13 @@ def main():
         "mixed_over_fp64": ms_fp64 / ms_mixed,
         "e2e": {"value": ws * nprob / (ms_e2e / 1e3), "unit": "solves/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
-        "roofline": {"kernel": "bsweep_tma (block L and U sweeps, FP32 values)",
+        "roofline": {"kernel": "bsweep_tma (block L and U sweeps, FP32 factor values)",
                      "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": peak_kind,
-                     "traffic": None, "levels": [inf["levels_L"], inf["levels_U"]],
-                     "problem": meshes[ib].name},
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "launches": sweep_launches,
+                     "ms_per_launch": sweep_ms / max(sweep_launches, 1),
+                     "algorithmic_bytes_per_launch": sweep_bytes / max(sweep_launches, 1),
+                     "share_of_step": sweep_ms / (ms_mixed * args.steps)},
         "clocks": clk,
         "gpu_launches": int(launches),
     }

@@ -93,6 +93,9 @@ SIGNATURES = {
     "gf_precond_factor": (_I, [_P, _P, _P]),
     "gf_precond_apply": (_I, [_P, _P, _P, _P]),
     "gf_precond_apply_noalloc": (_I, [_P, _P, _P, _P]),
+    "gf_timing_enable": (_I, [C.c_int32]),
+    "gf_timing_read": (_I, [C.POINTER(C.c_double), C.POINTER(C.c_longlong),
+                            C.POINTER(C.c_double)]),
     "gf_precond_info": (_I, [_P, _PI, _PI, _PI]),
     "gf_precond_get": (_I, [_P, _PI, _PI, _PD]),
     "gf_solve_opts_default": (None, [C.POINTER(gf_solve_opts)]),

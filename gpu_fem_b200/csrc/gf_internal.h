@@ -118,6 +118,7 @@ struct TriDesc {
   int capb, capr;                // blocks / rows per chunk at most
   const int64_t* off;            // [nch+1] byte offsets into stream
   const unsigned char* stream;
+  long long abytes;              // algorithmic bytes of one sweep (for timing)
 };
 
 // Per-problem descriptor used by the batched solver kernels: block rows,

@@ -34,13 +34,10 @@
 namespace gf {
 
 enum { ST_TIMEOUT = 1, ST_ZERO_PIVOT = 2, ST_NAN = 4 };
-constexpr int kCtaThreads = 1024;  // one CTA per problem for triangular work
 constexpr int kChunk = 4096;
 constexpr int kRedThreads = 256;
 
 struct SweepCtl {
-  int epoch;
-  int counter;
   int status;
   int pivot;
 };
@@ -133,62 +130,130 @@ __device__ void inv6_warp(double* M, double* Inv, int lane, SweepCtl* ctl, int r
 // IKJ block ILU on each problem's ILU pattern (FP64, in place): lower blocks
 // become L_ik = A_ik U_kk^{-1}, the diagonal block is replaced by U_ii^{-1}.
 // One CTA per problem walks the levels of the lower-triangular DAG; the
-// rows of a level are independent and spread over the warps, and levels are
+// rows of a level are independent, one warp per row, and levels are
 // separated by __syncthreads() (block-scope visibility of global writes).
-__global__ void __launch_bounds__(kCtaThreads) bfactor_cta(const ProbDev* __restrict__ P,
-                                                          SweepCtl* ctl) {
-  __shared__ double sm[kCtaThreads / 32][3][36];
+// Within a row the steps k (its lower blocks, ascending) are sequential; a
+// step's updates A_ij -= L_ik U_kj over j in U(k) are spread over the lanes
+// (lane = block slot b < 5, column c < 6; 4 slots batches in flight), and
+// the column lists and U_kj values of a batch are loaded together with
+// A_ik and U_kk^{-1} so a step costs about two memory latencies. Each row's
+// column indices are staged in shared memory for the searches j -> slot.
+constexpr int kFacWarps = 8;
+constexpr int kFacRow = 512;    // row blocks whose columns are staged in shared memory
+constexpr int kFacBatch = 4;    // update passes of 5 blocks in flight per lane
+
+__device__ __forceinline__ int find_col(const int32_t* c, int lo, int hi, int j) {
+  const int end = hi;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (c[mid] < j)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return (lo < end && c[lo] == j) ? lo : -1;
+}
+
+__global__ void __launch_bounds__(kFacWarps * 32) bfactor_kernel(const ProbDev* __restrict__ P,
+                                                                SweepCtl* ctl) {
+  __shared__ double sL[kFacWarps][36];
+  __shared__ double sM[kFacWarps][36];
+  __shared__ double sI[kFacWarps][36];
+  __shared__ int32_t sC[kFacWarps][kFacRow];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  double* Lb = sm[warp][0];
-  double* M = sm[warp][1];
-  double* Inv = sm[warp][2];
+  const int b = lane / 6, c = lane % 6;  // update slot and column (lanes 30, 31 idle)
   const ProbDev d = P[blockIdx.x];
   const int32_t* rowp = d.prowp;
   const int32_t* cols = d.pcols;
   const int32_t* diag = d.pdiag;
   double* LU = d.LU64;
+  double* Lb = sL[warp];
   for (int lev = 0; lev < d.nlevL; lev++) {
     for (int idx = d.levLptr[lev] + warp; idx < d.levLptr[lev + 1]; idx += nw) {
       const int i = d.levLrows[idx];
-      const int r1 = rowp[i + 1], di = diag[i];
-      for (int kp = rowp[i]; kp < di; kp++) {
-        const int k = cols[kp];
-        const double* Ukk = LU + 36 * (size_t)diag[k];
-        const double* Aik = LU + 36 * (size_t)kp;
-        for (int t = lane; t < 36; t += 32) {
-          const int r = t / 6, c = t % 6;
-          double s = 0.0;
+      const int r0 = rowp[i], r1 = rowp[i + 1], di = diag[i], len = r1 - r0;
+      const bool staged = len <= kFacRow;
+      const int32_t* rc = staged ? sC[warp] - r0 : cols;  // rc[kp] = column of slot kp
+      if (staged)
+        for (int t = lane; t < len; t += 32) sC[warp][t] = cols[r0 + t];
+      __syncwarp();
+      for (int kp = r0; kp < di; kp++) {
+        const int k = rc[kp];
+        const int u0 = diag[k] + 1, u1 = rowp[k + 1];
+        // loads that do not depend on this row's earlier steps: the first
+        // batch of U(k) columns and values, U_kk^{-1}
+        int jc[kFacBatch];
+        double u[kFacBatch][6];
 #pragma unroll
-          for (int m = 0; m < 6; m++) s = fma(Aik[6 * r + m], Ukk[6 * m + c], s);
-          Lb[t] = s;
+        for (int q = 0; q < kFacBatch; q++) {
+          const int jp = u0 + 5 * q + b;
+          jc[q] = (lane < 30 && jp < u1) ? cols[jp] : -1;
+          if (jc[q] >= 0)
+#pragma unroll
+            for (int m = 0; m < 6; m++) u[q][m] = LU[36 * (size_t)jp + 6 * m + c];
+        }
+        const double* Ukk = LU + 36 * (size_t)diag[k];
+        double* Aik = LU + 36 * (size_t)kp;
+        double s0 = 0.0, s1 = 0.0;
+        {
+          const int r = lane / 6, cc = lane % 6;
+#pragma unroll
+          for (int m = 0; m < 6; m++) s0 = fma(Aik[6 * r + m], Ukk[6 * m + cc], s0);
+          if (lane < 4) {
+            const int r2 = (lane + 32) / 6, c2 = (lane + 32) % 6;
+#pragma unroll
+            for (int m = 0; m < 6; m++) s1 = fma(Aik[6 * r2 + m], Ukk[6 * m + c2], s1);
+          }
         }
         __syncwarp();
-        for (int t = lane; t < 36; t += 32) LU[36 * (size_t)kp + t] = Lb[t];
-        int tp = kp + 1;
-        const int k1 = rowp[k + 1];
-        for (int jp = diag[k] + 1; jp < k1; jp++) {
-          const int j = cols[jp];
-          while (tp < r1 && cols[tp] < j) tp++;
-          if (tp >= r1) break;
-          if (cols[tp] != j) continue;
-          const double* Ukj = LU + 36 * (size_t)jp;
-          double* Aij = LU + 36 * (size_t)tp;
-          for (int t = lane; t < 36; t += 32) {
-            const int r = t / 6, c = t % 6;
-            double s = 0.0;
+        Lb[lane] = s0;
+        Aik[lane] = s0;
+        if (lane < 4) {
+          Lb[32 + lane] = s1;
+          Aik[32 + lane] = s1;
+        }
+        __syncwarp();
+        for (int jb = u0; jb < u1; jb += 5 * kFacBatch) {
+          if (jb != u0) {
 #pragma unroll
-            for (int m = 0; m < 6; m++) s = fma(Lb[6 * r + m], Ukj[6 * m + c], s);
-            Aij[t] -= s;
+            for (int q = 0; q < kFacBatch; q++) {
+              const int jp = jb + 5 * q + b;
+              jc[q] = (lane < 30 && jp < u1) ? cols[jp] : -1;
+              if (jc[q] >= 0)
+#pragma unroll
+                for (int m = 0; m < 6; m++) u[q][m] = LU[36 * (size_t)jp + 6 * m + c];
+            }
           }
+          int tp[kFacBatch];
+#pragma unroll
+          for (int q = 0; q < kFacBatch; q++)
+            tp[q] = jc[q] >= 0 ? find_col(rc, kp + 1, r1, jc[q]) : -1;
+          double a[kFacBatch][6];
+#pragma unroll
+          for (int q = 0; q < kFacBatch; q++)
+            if (tp[q] >= 0)
+#pragma unroll
+              for (int r = 0; r < 6; r++) a[q][r] = LU[36 * (size_t)tp[q] + 6 * r + c];
+#pragma unroll
+          for (int q = 0; q < kFacBatch; q++)
+            if (tp[q] >= 0) {
+#pragma unroll
+              for (int r = 0; r < 6; r++) {
+                double s = 0.0;
+#pragma unroll
+                for (int m = 0; m < 6; m++) s = fma(Lb[6 * r + m], u[q][m], s);
+                LU[36 * (size_t)tp[q] + 6 * r + c] = a[q][r] - s;
+              }
+            }
         }
         __syncwarp();
       }
       double* Dii = LU + 36 * (size_t)di;
-      for (int t = lane; t < 36; t += 32) M[t] = Dii[t];
+      for (int t = lane; t < 36; t += 32) sM[warp][t] = Dii[t];
       __syncwarp();
-      inv6_warp(M, Inv, lane, ctl, d.off + i);
+      inv6_warp(sM[warp], sI[warp], lane, ctl, d.off + i);
       for (int t = lane; t < 36; t += 32) {
-        const double v = Inv[t];
+        const double v = sI[warp][t];
         if (!isfinite(v)) {
           atomicOr(&ctl->status, ST_ZERO_PIVOT);
           atomicCAS(&ctl->pivot, 0, d.off + i + 1);
@@ -287,7 +352,8 @@ template <class VT, bool UPPER>
 __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __restrict__ P,
                                                            const int* __restrict__ live,
                                                            const double* __restrict__ rhs,
-                                                           double* out, SweepCtl* ctl) {
+                                                           double* out, SweepCtl* ctl,
+                                                           unsigned long long* bytes_ctr) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint64_t bar[kStages];
   __shared__ int abort_flag;
@@ -395,6 +461,7 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
       }
     }
   }
+  if (!abort_flag && tid == 0 && bytes_ctr) atomicAdd(bytes_ctr, (unsigned long long)T.abytes);
   if (abort_flag && tid == 0) {
     atomicOr(&ctl->status, ST_TIMEOUT);
     // chunks c .. issued-1 may still be in flight: let them land (bounded)
@@ -666,6 +733,7 @@ struct gf_precond {
   struct Tri {
     int nch = 0, stage = 0, capb = 0, capr = 0;
     size_t nslots = 0;
+    long long abytes = 0;
     DevBuf<int64_t> off, vpos;
     DevBuf<int32_t> map;
     DevBuf<unsigned char> stream;
@@ -760,7 +828,13 @@ static cudaError_t build_tri(gf_precond* p, const std::vector<int32_t>& diag, bo
     for (int k = 0; k < nb; k++) vpos[q + k] = v0 + 36 * (int64_t)k;
     q += nb;
   }
+  // algorithmic bytes of one sweep: per stored block its values, column
+  // index and the 6 x entries it multiplies; per row a row pointer, its
+  // right-hand side and its result
+  long long real = 0;
+  for (int i = 0; i < n; i++) real += cnt(i);
   gf_precond::Tri& t = p->tri[upper ? 1 : 0];
+  t.abytes = real * (36 * (long long)vs + 4 + 48) + (long long)n * (4 + 48 + 48);
   t.nch = nch;
   t.stage = stage;
   t.capb = capb;
@@ -778,7 +852,7 @@ static cudaError_t build_tri(gf_precond* p, const std::vector<int32_t>& diag, bo
 }
 static TriDesc tri_desc(const gf_precond* p, int which) {
   const gf_precond::Tri& t = p->tri[which];
-  return TriDesc{t.nch, t.stage, t.capb, t.capr, t.off.p, t.stream.p};
+  return TriDesc{t.nch, t.stage, t.capb, t.capr, t.off.p, t.stream.p, t.abytes};
 }
 static size_t sweep_smem(const gf_precond* p, int which) {
   const gf_precond::Tri& t = p->tri[which];
@@ -950,6 +1024,58 @@ static GmArrays arrays(gf_batch* B) {
 }
 
 
+// Sweep timing for benchmarks (gf_timing_enable / gf_timing_read): CUDA
+// events bracket the two sweep launches of every preconditioner apply on the
+// launching stream, and the sweeps add their algorithmic bytes to a device
+// counter. Off by default; the events come from a pool that is drained
+// (synchronised and summed) when it runs full.
+namespace {
+struct Timing {
+  std::mutex mu;
+  bool on = false;
+  unsigned long long* d_bytes = nullptr;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pool;
+  size_t used = 0;
+  double ms = 0.0;
+  long long launches = 0;
+};
+Timing g_timing;
+constexpr size_t kTimingPool = 8192;
+cudaError_t timing_drain_locked() {
+  for (size_t k = 0; k < g_timing.used; k++) {
+    float t = 0.f;
+    cudaError_t e = cudaEventSynchronize(g_timing.pool[k].second);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&t, g_timing.pool[k].first, g_timing.pool[k].second);
+    if (e != cudaSuccess) return e;
+    g_timing.ms += t;
+  }
+  g_timing.used = 0;
+  return cudaSuccess;
+}
+}  // namespace
+// Records the opening event of one sweep pair when timing is on; *e1 gets
+// the closing event to record after the second launch.
+static gf_status timing_begin(cudaStream_t st, unsigned long long** ctr, cudaEvent_t* e1) {
+  std::lock_guard<std::mutex> lk(g_timing.mu);
+  if (!g_timing.on) return GF_OK;
+  if (g_timing.used == g_timing.pool.size()) {
+    if (g_timing.pool.size() < kTimingPool) {
+      cudaEvent_t a, b;
+      GF_CUDA(cudaEventCreate(&a));
+      GF_CUDA(cudaEventCreate(&b));
+      g_timing.pool.emplace_back(a, b);
+    } else {
+      GF_CUDA(timing_drain_locked());
+    }
+  }
+  auto& pr = g_timing.pool[g_timing.used++];
+  GF_CUDA(cudaEventRecord(pr.first, st));
+  *e1 = pr.second;
+  *ctr = g_timing.d_bytes;
+  g_timing.launches += 2;
+  return GF_OK;
+}
+
 // z = U^{-1} L^{-1} r for problems with live[p] (all when live is null).
 // The factor values are in the preconditioners' precision (one per batch),
 // independent of the precision of the Krylov loop that calls this.
@@ -962,11 +1088,15 @@ static gf_status bsweeps(gf_batch* B, const int* live, const double* r, double* 
                                (int)kSweepSmemMax));
   GF_CUDA(cudaFuncSetAttribute(bsweep_tma<VT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)kSweepSmemMax));
+  unsigned long long* ctr = nullptr;
+  cudaEvent_t e1 = nullptr;
+  if (timing_begin(st, &ctr, &e1) != GF_OK) return GF_CUDA_ERROR;
   bsweep_tma<VT, false><<<B->np, kSweepThreads, B->smemL, st>>>(B->d_desc.p, live, r, B->d_tmp.p,
-                                                                B->d_ctl.p); ::gf::count_launch();
+                                                                B->d_ctl.p, ctr); ::gf::count_launch();
   bsweep_tma<VT, true><<<B->np, kSweepThreads, B->smemU, st>>>(B->d_desc.p, live, B->d_tmp.p, z,
-                                                               B->d_ctl.p); ::gf::count_launch();
+                                                               B->d_ctl.p, ctr); ::gf::count_launch();
   GF_CHECK_LAUNCH();
+  if (e1) GF_CUDA(cudaEventRecord(e1, st));
   return GF_OK;
 }
 template <class VT>
@@ -1003,7 +1133,7 @@ static gf_status batch_factor(gf_batch* B, cudaStream_t st) {
   }
   GF_CHECK_LAUNCH();
   GF_CUDA(cudaMemsetAsync(&B->d_ctl.p->status, 0, 2 * sizeof(int), st));
-  bfactor_cta<<<B->np, kCtaThreads, 0, st>>>(B->d_desc.p, B->d_ctl.p); ::gf::count_launch();
+  bfactor_kernel<<<B->np, kFacWarps * 32, 0, st>>>(B->d_desc.p, B->d_ctl.p); ::gf::count_launch();
   GF_CHECK_LAUNCH();
   for (int k = 0; k < B->np; k++) {
     gf_precond* p = B->pcs[k];
@@ -1466,10 +1596,10 @@ gf_status gf_precond_apply_noalloc(gf_precond* p, const double* d_r, double* d_z
     GF_CUDA(cudaFuncSetAttribute(bsweep_tma<float, true>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSweepSmemMax));
     bsweep_tma<float, false><<<1, kSweepThreads, B->smemL, st>>>(B->d_desc.p, nullptr, d_r, y,
-                                                                 B->d_ctl.p);
+                                                                 B->d_ctl.p, nullptr);
     ::gf::count_launch();
     bsweep_tma<float, true><<<1, kSweepThreads, B->smemU, st>>>(B->d_desc.p, nullptr, y, d_z,
-                                                                B->d_ctl.p);
+                                                                B->d_ctl.p, nullptr);
     ::gf::count_launch();
   } else {
     GF_CUDA(cudaFuncSetAttribute(bsweep_tma<double, false>,
@@ -1477,13 +1607,40 @@ gf_status gf_precond_apply_noalloc(gf_precond* p, const double* d_r, double* d_z
     GF_CUDA(cudaFuncSetAttribute(bsweep_tma<double, true>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSweepSmemMax));
     bsweep_tma<double, false><<<1, kSweepThreads, B->smemL, st>>>(B->d_desc.p, nullptr, d_r, y,
-                                                                  B->d_ctl.p);
+                                                                  B->d_ctl.p, nullptr);
     ::gf::count_launch();
     bsweep_tma<double, true><<<1, kSweepThreads, B->smemU, st>>>(B->d_desc.p, nullptr, y, d_z,
-                                                                 B->d_ctl.p);
+                                                                 B->d_ctl.p, nullptr);
     ::gf::count_launch();
   }
   GF_CHECK_LAUNCH();
+  return GF_OK;
+}
+
+gf_status gf_timing_enable(int32_t enable) {
+  std::lock_guard<std::mutex> lk(g_timing.mu);
+  GF_CUDA(timing_drain_locked());
+  g_timing.ms = 0.0;
+  g_timing.launches = 0;
+  if (enable && !g_timing.d_bytes) {
+    void* p = nullptr;
+    GF_CUDA(cudaMalloc(&p, sizeof(unsigned long long)));
+    g_timing.d_bytes = static_cast<unsigned long long*>(p);
+  }
+  if (g_timing.d_bytes) GF_CUDA(cudaMemset(g_timing.d_bytes, 0, sizeof(unsigned long long)));
+  g_timing.on = enable != 0;
+  return GF_OK;
+}
+
+gf_status gf_timing_read(double* sweep_ms, long long* sweep_launches, double* sweep_bytes) {
+  std::lock_guard<std::mutex> lk(g_timing.mu);
+  GF_CUDA(timing_drain_locked());
+  unsigned long long b = 0;
+  if (g_timing.d_bytes)
+    GF_CUDA(cudaMemcpy(&b, g_timing.d_bytes, sizeof(b), cudaMemcpyDeviceToHost));
+  if (sweep_ms) *sweep_ms = g_timing.ms;
+  if (sweep_launches) *sweep_launches = g_timing.launches;
+  if (sweep_bytes) *sweep_bytes = (double)b;
   return GF_OK;
 }
 

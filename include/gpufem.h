@@ -82,6 +82,17 @@ const char* gf_version(void);
 const char* gf_last_error(void);
 /* Number of kernels the library has launched in this process (all threads). */
 long long gf_launch_count(void);
+/* Sweep timing for benchmarks (no reference counterpart). While enabled,
+ * the two triangular-sweep launches of every preconditioner apply are
+ * bracketed by CUDA events on their stream, and the sweeps add their
+ * algorithmic bytes (stored blocks: 36 values + column index + 6 gathered x
+ * entries; rows: row pointer + right-hand side + result) to a device counter.
+ * Enabling or disabling resets the totals. Meant for a benchmark driving
+ * the library from one host thread. */
+gf_status gf_timing_enable(int32_t enable);
+/* Totals since the last enable: event time of the sweep pairs (ms), sweep
+ * launches and algorithmic bytes. Waits for the recorded events. */
+gf_status gf_timing_read(double* sweep_ms, long long* sweep_launches, double* sweep_bytes);
 
 /* ---- assembler ------------------------------------------------------- */
 /* ElementAssembler(...) (include/assembler.h:31-73) + BsrData(...)
