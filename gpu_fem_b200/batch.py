@@ -6,14 +6,19 @@ device-resident; a step re-assembles K (fused BCs) for every problem,
 refactors all preconditioners in one level-ordered launch and solves all
 problems together (gf_batch_*): one SpMV launch and one launch per
 triangular sweep for the whole batch, per-problem GMRES states. Precision:
-FP64, or FP32 ILU + FP32 SpMV inside FP64 iterative refinement (mixed).
+FP64, or FP32 ILU factors inside FP64 GMRES (mixed); FP32 ILU + FP32 SpMV
+inside FP64 iterative refinement is available as well.
 
 Autotuner: block ILU(0) is unstable on thin shells (Schur complements of the
 membrane-dominated rows lose definiteness), so the fill level k of the
 symbolic ILU(k) (computeILUk, include/linalg/bsr_utils.h:678-807) is chosen
 per problem: every candidate k is tried on the whole batch in one batched
-FP64 solve with an iteration cap, and each problem keeps the converging k
-with the smallest estimated sweep work (iterations x triangular levels).
+solve (FP32 factors, the less forgiving precision, inside FP64 GMRES) with
+an iteration cap, and each problem keeps the converging k
+with the smallest estimated critical path (iterations x triangular levels
+for the sweeps, lower levels x lower blocks per row for the factorization).
+The node ordering (natural or RCM) is chosen first, by levels x blocks per
+row of ILU(8).
 """
 from __future__ import annotations
 
@@ -73,14 +78,47 @@ def solve_opts(rtol=1e-8, mixed=False, restart=100, max_iters=20000, inner_rtol=
                         check_every=25)
 
 
+ORDERINGS = ("natural", "rcm")
+
+
+def choose_ordering(mesh, fill=8):
+    """Assembler of the mesh in the node ordering whose ILU(fill) triangles
+    have the fewest levels (the sweeps' critical path). Line-by-line
+    (natural) numbering of a structured plate gives levels ~ n_long +
+    (fill + 2) n_short, several times fewer than RCM's diagonal wavefronts,
+    whose nodes chain up through the element diagonals; RCM stays the choice
+    for meshes whose generator numbering is poor."""
+    best = None
+    for o in ORDERINGS:
+        a = ElementAssembler.from_mesh(mesh, ordering=o)
+        try:
+            inf = ILUk_Preconditioner(a, fill, "fp64").info()
+        except L.GpuFemError:  # fill rows too long for the sweep kernel
+            continue
+        # levels x blocks per row: both the sweep and the factorization
+        # critical paths grow with it (a poor numbering fills in heavily)
+        score = (inf["levels_L"] + inf["levels_U"]) * inf["nnzb"] / a.get_num_nodes()
+        if best is None or score < best[0]:
+            best = (score, o, a)
+    if best is None:
+        raise RuntimeError(f"no ordering of {mesh.name} gives a usable ILU({fill})")
+    return best[1], best[2]
+
+
 class BatchSolver:
     """Problems resident on the current device, solved as one batch."""
 
-    def __init__(self, meshes, ordering="rcm", tune=True, fill=None, rtol=1e-8, restart=100,
+    def __init__(self, meshes, ordering="auto", tune=True, fill=None, rtol=1e-8, restart=100,
                  build=True):
         self.rtol, self.restart = rtol, restart
         self.meshes = meshes
-        self.asms = [ElementAssembler.from_mesh(m, ordering=ordering) for m in meshes]
+        if ordering == "auto":
+            picked = [choose_ordering(m) for m in meshes]
+            self.orderings = [o for o, _ in picked]
+            self.asms = [a for _, a in picked]
+        else:
+            self.orderings = [ordering] * len(meshes)
+            self.asms = [ElementAssembler.from_mesh(m, ordering=ordering) for m in meshes]
         self.mats = [BsrMat(a) for a in self.asms]
         self.bs = [torch.tensor(m.loads, device="cuda") for m in meshes]
         self.xs = [torch.zeros_like(b) for b in self.bs]
@@ -110,7 +148,11 @@ class BatchSolver:
             todo = [i for i in range(n) if best[i] is None or k <= best[i][2] + 4]
             if not todo:
                 break
-            P = [ILUk_Preconditioner(self.asms[i], k, "fp64") for i in todo]
+            try:
+                P = [ILUk_Preconditioner(self.asms[i], k, "fp32") for i in todo]
+            except L.GpuFemError:  # a factor row longer than the sweep's stage
+                log.append((k, "precond create failed"))
+                break
             bt = Batch([self.asms[i] for i in todo], [self.mats[i] for i in todo], P)
             try:
                 bt.factor()
@@ -120,14 +162,20 @@ class BatchSolver:
             for i in todo:
                 self.xs[i].zero_()
             st, stats = bt.solve([self.bs[i] for i in todo], [self.xs[i] for i in todo],
-                                 solve_opts(self.rtol, False, restart=200, max_iters=cap))
+                                 solve_opts(self.rtol, False, restart=self.restart, max_iters=cap))
             for j, i in enumerate(todo):
                 s = stats[j]
-                nlev = P[j].info()["levels_L"] + P[j].info()["levels_U"]
+                inf = P[j].info()
+                nlev = inf["levels_L"] + inf["levels_U"]
                 ok = s["status"] == L.GF_OK
                 log.append((i, k, s["iterations"], s["rel_residual"], nlev, ok))
                 if ok:
-                    cost = s["iterations"] * nlev
+                    # critical-path model (microseconds): every iteration runs
+                    # both sweeps (~2 us a level); the factorization takes
+                    # ~1 us per lower block of a row along the lower levels
+                    nrow = self.asms[i].get_num_nodes()
+                    lower = max(inf["nnzb"] - nrow, 0) / (2.0 * nrow)
+                    cost = 2.0 * s["iterations"] * nlev + inf["levels_L"] * lower
                     if best[i] is None or cost < best[i][0]:
                         best[i] = (cost, k, k)
             if all(b is not None for b in best) and k >= max(b[1] for b in best) + 4:
@@ -137,8 +185,12 @@ class BatchSolver:
             raise RuntimeError(f"no ILU fill level converged for {missing}")
         return [b[1] for b in best], log
 
-    def step(self, mixed: bool, host_io=None):
-        """Assemble, factor and solve every problem once."""
+    def step(self, mixed: bool, host_io=None, spmv32=False):
+        """Assemble, factor and solve every problem once. mixed: FP32 ILU
+        factors (half the bytes of the sweeps' factor streams) inside FP64
+        GMRES; with spmv32 also FP32 SpMV in an inner GMRES under FP64
+        iterative refinement, whose reachable residual is limited by
+        cond(A) x 6e-8 and so fails on the thinnest shells."""
         if host_io is not None:
             for b, hb in zip(self.bs, host_io[0]):
                 b.copy_(hb, non_blocking=True)
@@ -147,7 +199,8 @@ class BatchSolver:
         bt.factor()
         for x in self.xs:
             x.zero_()
-        st, stats = bt.solve(self.bs, self.xs, solve_opts(self.rtol, mixed, self.restart))
+        st, stats = bt.solve(self.bs, self.xs,
+                             solve_opts(self.rtol, mixed and spmv32, self.restart))
         if st != L.GF_OK:
             raise RuntimeError(f"batch solve failed: {[s for s in stats if s['status']]}")
         if host_io is not None:

@@ -280,21 +280,23 @@ __global__ void convert_kernel(size_t n, const double* __restrict__ in, T2* __re
 
 
 // ------------------------------------------- prefetched level-major sweeps
-// One CTA per problem walks the chunks of one triangle in level-major order.
-// A ring of kStages shared-memory buffers is filled by 1D bulk copies
-// (cp.async.bulk, completion counted on an mbarrier) kStages-1 chunks ahead
-// of the chunk being solved, so the HBM latency of the factor values is off
-// the critical path. Per chunk: wait for its stage, gather the x entries its
-// blocks multiply into shared memory (one parallel round of loads), then
-// solve its rows, spread over the warps (a chunk never spans two levels).
-// x / y live in global memory, written and re-read by this CTA only; two
-// block barriers per chunk order the gather after the previous chunk's
-// writes and the solve after the gather.
+// One CTA per problem walks the chunks of one triangle in level-major order
+// (a chunk holds rows of one level). A ring of kStages shared-memory stages
+// is filled by 1D bulk copies (cp.async.bulk, completion counted on an
+// mbarrier) kStages-1 chunks ahead, so the factor values are never waited
+// for. The x entries a chunk multiplies come from two places:
+//  - near: rows solved by the previous chunk, kept in a shared-memory ring;
+//  - far: rows solved two or more chunks earlier, loaded from global memory
+//    one chunk ahead (issued right after the barrier that ends chunk c-1,
+//    consumed by chunk c+1), together with chunk c+1's right-hand sides;
+// so a chunk's critical path is two block barriers, shared-memory copies and
+// its rows' 6x6 products. x / y live in global memory, written and re-read
+// by this CTA only.
 constexpr int kSweepThreads = 512;
-constexpr int kStages = 3;
+constexpr int kStages = 4;
 constexpr unsigned long long kWaitNs = 2000000000ull;
 constexpr size_t kSweepSmemMax = 220 * 1024;  // dynamic; the static part is < 1 KB
-constexpr int kGather = 8;  // gathered values per thread and chunk: 6 (capb + capr) <= 4096
+constexpr int kGather = 8;  // prefetched values per thread and chunk: 6 (capb + capr) <= 4096
 
 __device__ __forceinline__ unsigned long long gtimer() {
   unsigned long long t;
@@ -342,10 +344,10 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
 }
 
 // Dynamic shared memory of one sweep: kStages staging buffers of `stage`
-// bytes, then the gathered x of one chunk (capb x 6 doubles) and its
-// right-hand sides (capr x 6 doubles).
+// bytes; the gathered x of one chunk (capb x 6 doubles) and its right-hand
+// sides (capr x 6); the ring of the two latest chunks' results (2 capr x 6).
 __host__ __device__ inline size_t sweep_smem_bytes(int stage, int capb, int capr) {
-  return kStages * (size_t)stage + 48 * ((size_t)capb + capr);
+  return kStages * (size_t)stage + 48 * ((size_t)capb + 3 * (size_t)capr);
 }
 
 template <class VT, bool UPPER>
@@ -363,8 +365,9 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
   const int g = lane / 6, r = lane % 6;
   const ProbDev& d = P[p];
   const TriDesc T = UPPER ? d.U : d.L;
-  double* xs = reinterpret_cast<double*>(smem + (size_t)kStages * T.stage);
-  double* rs = xs + 6 * (size_t)T.capb;
+  double* xs = reinterpret_cast<double*>(smem + (size_t)kStages * T.stage);  // capb x 6
+  double* rs = xs + 6 * (size_t)T.capb;                                      // capr x 6
+  double* ring = rs + 6 * (size_t)T.capr;                                    // 2 x capr x 6
   const double* rb = rhs + 6 * (size_t)d.off;
   double* ob = out + 6 * (size_t)d.off;
   if (tid == 0) {
@@ -389,11 +392,31 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
   if (tid == 0)
     for (int c = 0; c < kStages - 1 && c < T.nch; c++) issue(c);
   int issued = min(kStages - 1, T.nch);
+  // values waiting to be stored into xs / rs (destination index, -1: none)
+  double vcur[kGather];
+  int dcur[kGather];
+#pragma unroll
+  for (int u = 0; u < kGather; u++) dcur[u] = -1;
+  // chunk 0 has no earlier rows: only its right-hand sides
+  if (!mbar_wait(&bar[0], 0u)) abort_flag = 1;
+  __syncthreads();
+  if (!abort_flag) {
+    const int nr0 = reinterpret_cast<const int4*>(smem)->x;
+    const int4* ri0 = reinterpret_cast<const int4*>(smem + 32);
+#pragma unroll
+    for (int u = 0; u < kGather; u++) {
+      const int t = tid + u * kSweepThreads;
+      if (t < 6 * nr0) {
+        vcur[u] = rb[6 * (size_t)ri0[t / 6].x + t % 6];
+        dcur[u] = 6 * T.capb + t;
+      }
+    }
+  }
   int c = 0;
   for (; c < T.nch; c++) {
     const int s = c % kStages;
-    if (!mbar_wait(&bar[s], (unsigned)((c / kStages) & 1))) abort_flag = 1;
-    __syncthreads();  // chunk c-1's x writes done; its stage is free again
+    if (c > 0 && !mbar_wait(&bar[s], (unsigned)((c / kStages) & 1))) abort_flag = 1;
+    __syncthreads();  // chunk c-1 solved; its stage is free again
     if (abort_flag) break;
     if (issued < T.nch) {
       if (tid == 0) {
@@ -403,34 +426,46 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
       issued++;
     }
     const unsigned char* st = smem + (size_t)s * T.stage;
-    const int4 hdr = *reinterpret_cast<const int4*>(st);
-    const int nr = hdr.x, nb = hdr.y;
-    const int4* ri = reinterpret_cast<const int4*>(st + 16);
-    const int32_t* sc = reinterpret_cast<const int32_t*>(st + 16 + 16 * (size_t)nr);
-    const VT* sv = reinterpret_cast<const VT*>(st + 16 + 16 * (size_t)nr + 4 * (size_t)nb);
-    {
-      // every thread issues all its loads (x of the chunk's columns, then
-      // the rows' right-hand sides) before storing any: one memory latency
-      // per chunk instead of one per loop trip
-      double v[kGather];
+    const int4 h0 = reinterpret_cast<const int4*>(st)[0];
+    const int4 h1 = reinterpret_cast<const int4*>(st)[1];
+    const int nr = h0.x, nb = h0.y, nn = h0.z, nf1 = h1.x, nr1 = h1.y;
+    const int4* ri = reinterpret_cast<const int4*>(st + 32);
+    const int2* nearl = reinterpret_cast<const int2*>(ri + nr);
+    const int2* far1 = nearl + nn;
+    const int32_t* rows1 = reinterpret_cast<const int32_t*>(far1 + nf1);
+    const size_t voff = (32 + 16 * (size_t)nr + 8 * (size_t)(nn + nf1) + 4 * (size_t)nr1 + 15) &
+                        ~(size_t)15;
+    const VT* sv = reinterpret_cast<const VT*>(st + voff);
+    // loads for chunk c+1: far x entries (rows solved by chunks <= c-1, all
+    // complete at the barrier above) and right-hand sides
+    double vnxt[kGather];
+    int dnxt[kGather];
 #pragma unroll
-      for (int u = 0; u < kGather; u++) {
-        const int t = tid + u * kSweepThreads;
-        if (t < 6 * nb)
-          v[u] = ob[6 * (size_t)sc[t / 6] + t % 6];
-        else if (t < 6 * (nb + nr))
-          v[u] = rb[6 * (size_t)ri[t / 6 - nb].x + t % 6];
-      }
-#pragma unroll
-      for (int u = 0; u < kGather; u++) {
-        const int t = tid + u * kSweepThreads;
-        if (t < 6 * nb)
-          xs[t] = v[u];
-        else if (t < 6 * (nb + nr))
-          rs[t - 6 * nb] = v[u];
+    for (int u = 0; u < kGather; u++) {
+      const int t = tid + u * kSweepThreads;
+      dnxt[u] = -1;
+      if (t < 6 * nf1) {
+        const int2 f = far1[t / 6];
+        vnxt[u] = ob[6 * (size_t)f.y + t % 6];
+        dnxt[u] = 6 * f.x + t % 6;
+      } else if (t < 6 * (nf1 + nr1)) {
+        const int t2 = t - 6 * nf1;
+        vnxt[u] = rb[6 * (size_t)rows1[t2 / 6] + t2 % 6];
+        dnxt[u] = 6 * T.capb + t2;
       }
     }
+    // chunk c's far entries and right-hand sides, loaded one chunk ago
+#pragma unroll
+    for (int u = 0; u < kGather; u++)
+      if (dcur[u] >= 0) xs[dcur[u]] = vcur[u];
+    // near entries: results of chunk c-1 from the ring
+    const double* rp = ring + 6 * (size_t)T.capr * ((c + 1) & 1);
+    for (int t = tid; t < 6 * nn; t += kSweepThreads) {
+      const int2 q = nearl[t / 6];
+      xs[6 * q.x + t % 6] = rp[6 * q.y + t % 6];
+    }
     __syncthreads();
+    double* wp = ring + 6 * (size_t)T.capr * (c & 1);
     for (int k = warp; k < nr; k += nw) {
       const int4 row = ri[k];
       const int i = row.x, rbeg = row.y, rcnt = row.z;
@@ -447,18 +482,25 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
       acc += __shfl_down_sync(0xffffffffu, acc, 12);
       acc += __shfl_down_sync(0xffffffffu, acc, 6);
       const double t = (lane < 6 ? rs[6 * k + lane] : 0.0) - acc;
-      if (!UPPER) {
-        if (lane < 6) ob[6 * (size_t)i + lane] = t;
-      } else {
+      double v = t;
+      if (UPPER) {
         const VT* Di = sv + (size_t)rbeg * 36;
-        double v = 0.0;
+        v = 0.0;
 #pragma unroll
         for (int cc = 0; cc < 6; cc++) {
           const double tc = __shfl_sync(0xffffffffu, t, cc);
           if (lane < 6) v = fma((double)Di[6 * lane + cc], tc, v);
         }
-        if (lane < 6) ob[6 * (size_t)i + lane] = v;
       }
+      if (lane < 6) {
+        ob[6 * (size_t)i + lane] = v;
+        wp[6 * k + lane] = v;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kGather; u++) {
+      vcur[u] = vnxt[u];
+      dcur[u] = dnxt[u];
     }
   }
   if (!abort_flag && tid == 0 && bytes_ctr) atomicAdd(bytes_ctr, (unsigned long long)T.abytes);
@@ -759,7 +801,7 @@ static cudaError_t build_tri(gf_precond* p, const std::vector<int32_t>& diag, bo
   }
   int maxc = 0;
   for (int i = 0; i < n; i++) maxc = std::max(maxc, cnt(i));
-  const int capb = std::max(p->prec == GF_PREC_FP32 ? 320 : 192, (maxc + 3) & ~3);
+  const int capb = std::max(p->prec == GF_PREC_FP32 ? 256 : 128, (maxc + 3) & ~3);
   const int capr = 128;
   // pass 1: chunk boundaries (row ranges of `rows`) and block counts
   std::vector<int32_t> ck{0}, cb;  // chunk row starts, padded block counts
@@ -782,49 +824,95 @@ static cudaError_t build_tri(gf_precond* p, const std::vector<int32_t>& diag, bo
     }
   }
   const int nch = (int)cb.size();
+  // chunk and chunk-local index of every row
+  std::vector<int32_t> chunk_of(n), local(n);
+  for (int c = 0; c < nch; c++)
+    for (int k = ck[c]; k < ck[c + 1]; k++) {
+      chunk_of[rows[k]] = c;
+      local[rows[k]] = k - ck[c];
+    }
+  // per chunk: where each stored block's x comes from. Near: row solved by
+  // the previous chunk (ring, chunk-local row); far: solved earlier (global
+  // row). U's diagonal block U_ii^{-1} multiplies no x; padding is unused.
+  std::vector<std::vector<int32_t>> nearl(nch), farl(nch);  // pairs (slot, source)
+  for (int c = 0; c < nch; c++) {
+    int b = 0;
+    auto src = [&](int slot, int j) {
+      const int pc = chunk_of[j];
+      if (pc == c - 1) {
+        nearl[c].push_back(slot);
+        nearl[c].push_back(local[j]);
+      } else {
+        farl[c].push_back(slot);
+        farl[c].push_back(j);
+      }
+    };
+    for (int k = ck[c]; k < ck[c + 1]; k++) {
+      const int i = rows[k];
+      if (upper) {
+        b++;  // U_ii^{-1}
+        for (int jp = diag[i] + 1; jp < P.rowp[i + 1]; jp++) src(b++, P.cols[jp]);
+      } else {
+        for (int jp = P.rowp[i]; jp < diag[i]; jp++) src(b++, P.cols[jp]);
+      }
+    }
+  }
+  if (!farl[0].empty() || !nearl[0].empty()) return cudaErrorInvalidValue;  // level 0 has none
+  // byte layout of chunk c: two int4 headers, row records, near list, the
+  // far list and row indices of chunk c+1, then (16-byte aligned) values
+  auto pre = [&](int c) {
+    const int64_t nr = ck[c + 1] - ck[c];
+    const int64_t nf1 = c + 1 < nch ? (int64_t)farl[c + 1].size() / 2 : 0;
+    const int64_t nr1 = c + 1 < nch ? ck[c + 2] - ck[c + 1] : 0;
+    return (32 + 16 * nr + 4 * (int64_t)nearl[c].size() + 8 * nf1 + 4 * nr1 + 15) & ~(int64_t)15;
+  };
   std::vector<int64_t> off(nch + 1, 0);
   size_t nslots = 0;
   int stage = 0;
   for (int c = 0; c < nch; c++) {
-    const int nr = ck[c + 1] - ck[c];
-    const int64_t bytes = 16 + 16 * (int64_t)nr + (4 + 36 * (int64_t)vs) * cb[c];
+    const int64_t bytes = pre(c) + 36 * (int64_t)vs * cb[c];
     off[c + 1] = off[c] + bytes;
     stage = std::max<int64_t>(stage, bytes);
     nslots += cb[c];
   }
-  // pass 2: headers, row records, columns; value positions and sources
   std::vector<unsigned char> bytes(off[nch], 0);
   std::vector<int32_t> map(nslots, -1);
   std::vector<int64_t> vpos(nslots);
   size_t q = 0;
   for (int c = 0; c < nch; c++) {
-    unsigned char* base = bytes.data() + off[c];
+    int32_t* w = reinterpret_cast<int32_t*>(bytes.data() + off[c]);
     const int nr = ck[c + 1] - ck[c], nb = cb[c];
-    int32_t* hdr = reinterpret_cast<int32_t*>(base);
-    int32_t* rec = hdr + 4;
-    int32_t* col = rec + 4 * nr;
-    const int64_t v0 = (off[c] + 16 + 16 * (int64_t)nr + 4 * (int64_t)nb) / (int64_t)vs;
-    hdr[0] = nr;
-    hdr[1] = nb;
+    const int nn = (int)nearl[c].size() / 2;
+    const int nf1 = c + 1 < nch ? (int)farl[c + 1].size() / 2 : 0;
+    const int nr1 = c + 1 < nch ? ck[c + 2] - ck[c + 1] : 0;
+    w[0] = nr;
+    w[1] = nb;
+    w[2] = nn;
+    w[4] = nf1;
+    w[5] = nr1;
+    int32_t* rec = w + 8;
     int b = 0;
     for (int k = ck[c]; k < ck[c + 1]; k++) {
       const int i = rows[k];
       rec[4 * (k - ck[c]) + 0] = i;
       rec[4 * (k - ck[c]) + 1] = b;
       rec[4 * (k - ck[c]) + 2] = cnt(i);
-      auto put = [&](int jp) {
-        col[b] = P.cols[jp];
-        map[q + b] = jp;
-        b++;
-      };
       if (upper) {
-        put(diag[i]);
-        for (int jp = diag[i] + 1; jp < P.rowp[i + 1]; jp++) put(jp);
+        map[q + b++] = diag[i];
+        for (int jp = diag[i] + 1; jp < P.rowp[i + 1]; jp++) map[q + b++] = jp;
       } else {
-        for (int jp = P.rowp[i]; jp < diag[i]; jp++) put(jp);
+        for (int jp = P.rowp[i]; jp < diag[i]; jp++) map[q + b++] = jp;
       }
     }
-    for (int k = b; k < nb; k++) col[k] = 0;  // padding (never referenced by a row)
+    int32_t* lists = rec + 4 * nr;
+    std::copy(nearl[c].begin(), nearl[c].end(), lists);
+    lists += nearl[c].size();
+    if (c + 1 < nch) {
+      std::copy(farl[c + 1].begin(), farl[c + 1].end(), lists);
+      lists += farl[c + 1].size();
+      for (int k = ck[c + 1]; k < ck[c + 2]; k++) *lists++ = rows[k];
+    }
+    const int64_t v0 = (off[c] + pre(c)) / (int64_t)vs;
     for (int k = 0; k < nb; k++) vpos[q + k] = v0 + 36 * (int64_t)k;
     q += nb;
   }
@@ -1404,8 +1492,11 @@ static gf_status batch_solve_space(gf_batch* B, const gf_solve_opts& o,
       std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   for (int p = 0; p < np; p++) {
     S[p].time_ms = ms;
+    // hard failures (NaN, CUDA, timeout) mark every problem; otherwise each
+    // problem's status is its own convergence
     gf_status sp = result;
-    if (sp == GF_OK && !(S[p].rel_residual <= o.rtol)) sp = GF_NOT_CONVERGED;
+    if (sp == GF_OK || sp == GF_NOT_CONVERGED)
+      sp = (S[p].rel_residual <= o.rtol) ? GF_OK : GF_NOT_CONVERGED;
     S[p].status = sp;
     if (result == GF_OK && sp != GF_OK) result = sp;
   }

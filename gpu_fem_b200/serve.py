@@ -3,7 +3,7 @@
 Requests (a plate or a stiffened box, a size class, a per-request thickness
 field and load, all generated from the request seed) arrive as a Poisson
 stream. The server keeps, per size class, one device-resident assembler
-(mesh, BSR pattern, RCM ordering, coloured scatter schedule) and a pool of
+(mesh, node ordering, BSR pattern, coloured scatter schedule) and a pool of
 slots (BSR matrix, ILU(k) symbolic + factors, load / displacement vectors).
 A request is admitted when its slot memory fits the HBM budget; admitted
 requests are batched and solved with the batched engine (gf_batch_*) on a
@@ -13,6 +13,8 @@ up, and their work overlaps on the device. Latency = completion - arrival.
 
 Each request is solved with its own per-problem GMRES state and reductions,
 so its result does not depend on what else is in the batch (tested).
+Precision: FP32 ILU(k) factors inside FP64 GMRES; the fill level is tuned
+per size class at the thinnest thickness a request can carry.
 """
 from __future__ import annotations
 
@@ -28,7 +30,7 @@ import torch
 from . import _lib as L
 from . import mesh as M
 from .assembler import BsrMat, ElementAssembler, ILUk_Preconditioner, _stream
-from .batch import Batch, BatchSolver, solve_opts
+from .batch import Batch, BatchSolver, choose_ordering, solve_opts
 
 import ctypes as C
 
@@ -51,13 +53,14 @@ def class_mesh(family, dof):
 T_MIN = 0.0015
 
 
-def tune_class_fill(mesh, rtol=1e-8, margin=2):
+def tune_class_fill(mesh, ordering, rtol=1e-8, margin=2):
     """ILU fill level of a size class: the batch autotuner's choice at the
     thinnest thickness any request of the class can carry (the hardest case
     for block ILU on shells), plus a margin, so every request converges."""
     import dataclasses
     m = dataclasses.replace(mesh, thick=np.full(mesh.num_elements, T_MIN))
-    return BatchSolver([m], tune=True, rtol=rtol, build=False).fills[0] + margin
+    return BatchSolver([m], ordering=ordering, tune=True, rtol=rtol,
+                       build=False).fills[0] + margin
 
 
 @dataclass
@@ -96,17 +99,17 @@ def poisson_requests(rate, duration, seed=99, nclasses=16, families=("plate", "b
 
 
 class SizeClass:
-    def __init__(self, family, k, dof, fill):
+    def __init__(self, family, k, dof, fill=None, rtol=1e-8):
         self.family, self.k = family, k
         self.mesh = class_mesh(family, dof)
-        self.asm = ElementAssembler.from_mesh(self.mesh, ordering="rcm")
-        self.fill = fill
+        self.ordering, self.asm = choose_ordering(self.mesh)
+        self.fill = fill if fill is not None else tune_class_fill(self.mesh, self.ordering, rtol)
         self.free = []
         self.lock = threading.Lock()
         nn, ne = self.mesh.num_nodes, self.mesh.num_elements
         # per-slot footprint estimate: FP64+FP32 matrix, FP64+FP32 factors, vectors
         nnzb = self.asm.get_nnzb()
-        self.slot_bytes = int(nnzb * 36 * 12 * (1 + 1.5 * (fill > 0)) * 2 + 6 * nn * 8 * 8 +
+        self.slot_bytes = int(nnzb * 36 * 12 * (1 + 1.5 * (self.fill > 0)) * 2 + 6 * nn * 8 * 8 +
                               ne * 8)
 
     def make_slot(self):
@@ -153,9 +156,8 @@ class Server:
         key = (family, k)
         if key not in self.classes:
             dof = size_classes()[k]
-            if key not in self.fills:
-                self.fills[key] = tune_class_fill(class_mesh(family, dof), self.rtol)
-            self.classes[key] = SizeClass(family, k, dof, self.fills[key])
+            self.classes[key] = SizeClass(family, k, dof, self.fills.get(key), self.rtol)
+            self.fills[key] = self.classes[key].fill
         return self.classes[key]
 
     def warm(self, keys, slots=1):
@@ -203,7 +205,7 @@ class Server:
         L.check(L.lib().gf_batch_assemble_ex(bt.h, T, _stream()), "assemble")
         bt.factor()
         st, stats = bt.solve([s["b"] for _, _, s in batch], [s["x"] for _, _, s in batch],
-                             solve_opts(self.rtol, True, self.restart, self.max_iters))
+                             solve_opts(self.rtol, False, self.restart, self.max_iters))
         torch.cuda.current_stream().synchronize()
         now = time.perf_counter()
         for (req, _, slot), s in zip(batch, stats):

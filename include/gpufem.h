@@ -213,8 +213,10 @@ typedef struct gf_solve_opts {
   int32_t max_iters;      /* total Arnoldi steps */
   double rtol;            /* ||b - A x||_2 / ||b||_2 target (FP64 A) */
   int32_t side;           /* 0 left (reference), 1 right preconditioning */
-  int32_t mixed;          /* 0: FP64 GMRES; 1: FP32 SpMV + FP32 ILU inside
-                              FP64 GMRES with FP64 iterative refinement */
+  int32_t mixed;          /* 0: FP64 GMRES and SpMV (the preconditioner
+                              applies in its own precision, FP64 or FP32
+                              factors); 1: FP32 SpMV + FP32 ILU inside an
+                              inner GMRES under FP64 iterative refinement */
   double inner_rtol;      /* inner tolerance per refinement step (mixed) */
   int32_t max_refine;     /* max refinement steps (mixed) */
   int32_t check_every;    /* host polls convergence every k steps */

@@ -18,14 +18,15 @@ def _meshes():
                     lambda q: 1.5e3 + 0 * q[:, 0], name="p16x24")]
 
 
-@pytest.mark.parametrize("mixed", [False, True])
-def test_batch_alone_equals_mix_and_matches_dense(oracle, mixed):
+@pytest.mark.parametrize("mode", ["fp64", "mixed", "mixed_spmv32"])
+def test_batch_alone_equals_mix_and_matches_dense(oracle, mode):
     import torch
     from gpu_fem_b200.assembler import ILUk_Preconditioner, gmres_solve
     from gpu_fem_b200.batch import BatchSolver, solve_opts
     meshes = _meshes()
     bs = BatchSolver(meshes, fill=3)
-    stats = bs.step(mixed)
+    mixed, spmv32 = mode != "fp64", mode == "mixed_spmv32"
+    stats = bs.step(mixed, spmv32=spmv32)
     x_mix = [x.cpu().numpy().copy() for x in bs.xs]
     for i, m in enumerate(meshes):
         assert stats[i]["rel_residual"] <= 1e-8, stats[i]
@@ -34,7 +35,7 @@ def test_batch_alone_equals_mix_and_matches_dense(oracle, mixed):
         P.factor(bs.mats[i])
         x = torch.zeros_like(bs.bs[i])
         st, s1 = gmres_solve(bs.asms[i], bs.mats[i], P, bs.bs[i], x,
-                             solve_opts(1e-8, mixed, bs.restart))
+                             solve_opts(1e-8, spmv32, bs.restart))
         xa = x.cpu().numpy()
         assert np.array_equal(xa.view(np.uint64), x_mix[i].view(np.uint64)), (
             m.name, np.abs(xa - x_mix[i]).max())
