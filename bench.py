@@ -279,6 +279,8 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
+    timed_phases = []
+
     def timed(mixed, host_io=None, sweep_timing=False):
         import ctypes as C
         for _ in range(args.warmup):
@@ -291,10 +293,19 @@ def main():
         torch.cuda.nvtx.range_push("timed")
         ev[0].record()
         its = []
+        phase_ms = [0.0, 0.0, 0.0]
         for k in range(args.steps):
-            stats = bs.step(mixed, host_io)
+            pe = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            stats = bs.step(mixed, host_io, phases=pe)
             ev[k + 1].record()
             its.append(max(s["iterations"] for s in stats))
+            timed_phases.append(pe)
+        torch.cuda.synchronize()
+        for pe in timed_phases:
+            for q in range(3):
+                phase_ms[q] += pe[q].elapsed_time(pe[q + 1]) / args.steps
+        timed_phases.clear()
+        timed.phases = phase_ms
         barrier()
         torch.cuda.nvtx.range_pop()
         timed.launches = L.lib().gf_launch_count() - c0
@@ -318,6 +329,7 @@ def main():
     ms_mixed, lat_mixed = timed(True, sweep_timing=True)
     launches = timed.launches
     sweep_ms, sweep_launches, sweep_bytes = timed.sweep
+    phases_mixed = timed.phases
     its_mixed = timed.iters
     clk = clocks.stop()
     ms_fp64, lat_fp64 = timed(False)
@@ -356,6 +368,8 @@ def main():
                      "latency_ms": {"p50": float(np.percentile(lat_fp64, 50)),
                                     "p99": float(np.percentile(lat_fp64, 99))}},
         "mixed_over_fp64": ms_fp64 / ms_mixed,
+        "phase_ms": {"assemble": phases_mixed[0], "factor": phases_mixed[1],
+                     "solve": phases_mixed[2]},
         "e2e": {"value": ws * nprob / (ms_e2e / 1e3), "unit": "solves/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
         "roofline": {"kernel": "bsweep_tma (block L and U sweeps, FP32 factor values)",

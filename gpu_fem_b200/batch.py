@@ -185,22 +185,33 @@ class BatchSolver:
             raise RuntimeError(f"no ILU fill level converged for {missing}")
         return [b[1] for b in best], log
 
-    def step(self, mixed: bool, host_io=None, spmv32=False):
+    def step(self, mixed: bool, host_io=None, spmv32=False, phases=None):
         """Assemble, factor and solve every problem once. mixed: FP32 ILU
         factors (half the bytes of the sweeps' factor streams) inside FP64
         GMRES; with spmv32 also FP32 SpMV in an inner GMRES under FP64
         iterative refinement, whose reachable residual is limited by
-        cond(A) x 6e-8 and so fails on the thinnest shells."""
+        cond(A) x 6e-8 and so fails on the thinnest shells. phases: optional
+        list of 4 CUDA events recorded before assembly, factorization, solve
+        and after the solve."""
+        ev = phases if phases is not None else [None] * 4
         if host_io is not None:
             for b, hb in zip(self.bs, host_io[0]):
                 b.copy_(hb, non_blocking=True)
         bt = self.b32 if mixed else self.b64
+        if ev[0] is not None:
+            ev[0].record()
         bt.assemble()
+        if ev[1] is not None:
+            ev[1].record()
         bt.factor()
+        if ev[2] is not None:
+            ev[2].record()
         for x in self.xs:
             x.zero_()
         st, stats = bt.solve(self.bs, self.xs,
                              solve_opts(self.rtol, mixed and spmv32, self.restart))
+        if ev[3] is not None:
+            ev[3].record()
         if st != L.GF_OK:
             raise RuntimeError(f"batch solve failed: {[s for s in stats if s['status']]}")
         if host_io is not None:

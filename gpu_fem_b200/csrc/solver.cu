@@ -134,13 +134,13 @@ __device__ void inv6_warp(double* M, double* Inv, int lane, SweepCtl* ctl, int r
 // separated by __syncthreads() (block-scope visibility of global writes).
 // Within a row the steps k (its lower blocks, ascending) are sequential; a
 // step's updates A_ij -= L_ik U_kj over j in U(k) are spread over the lanes
-// (lane = block slot b < 5, column c < 6; 4 slots batches in flight), and
+// (lane = block slot b < 5, column c < 6; 2 slot batches in flight), and
 // the column lists and U_kj values of a batch are loaded together with
 // A_ik and U_kk^{-1} so a step costs about two memory latencies. Each row's
 // column indices are staged in shared memory for the searches j -> slot.
-constexpr int kFacWarps = 8;
-constexpr int kFacRow = 512;    // row blocks whose columns are staged in shared memory
-constexpr int kFacBatch = 4;    // update passes of 5 blocks in flight per lane
+constexpr int kFacWarps = 16;
+constexpr int kFacRow = 256;    // row blocks whose columns are staged in shared memory
+constexpr int kFacBatch = 2;    // update passes of 5 blocks in flight per lane
 
 __device__ __forceinline__ int find_col(const int32_t* c, int lo, int hi, int j) {
   const int end = hi;
@@ -296,7 +296,6 @@ constexpr int kSweepThreads = 512;
 constexpr int kStages = 4;
 constexpr unsigned long long kWaitNs = 2000000000ull;
 constexpr size_t kSweepSmemMax = 220 * 1024;  // dynamic; the static part is < 1 KB
-constexpr int kGather = 8;  // prefetched values per thread and chunk: 6 (capb + capr) <= 4096
 
 __device__ __forceinline__ unsigned long long gtimer() {
   unsigned long long t;
@@ -344,10 +343,48 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
 }
 
 // Dynamic shared memory of one sweep: kStages staging buffers of `stage`
-// bytes; the gathered x of one chunk (capb x 6 doubles) and its right-hand
-// sides (capr x 6); the ring of the two latest chunks' results (2 capr x 6).
+// bytes; two buffers (this chunk, next chunk) of gathered x (capb x 6
+// doubles) and right-hand sides (capr x 6); the ring of the two latest
+// chunks' results (2 capr x 6).
 __host__ __device__ inline size_t sweep_smem_bytes(int stage, int capb, int capr) {
-  return kStages * (size_t)stage + 48 * ((size_t)capb + 3 * (size_t)capr);
+  return kStages * (size_t)stage + 96 * ((size_t)capb + 2 * (size_t)capr);
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
+// Row r of a 6x6 block (6 consecutive values) times 6 x entries, with
+// vector shared-memory loads and two partial sums.
+__device__ __forceinline__ double dot6(const double* a, const double* x) {
+  const double2 a0 = reinterpret_cast<const double2*>(a)[0], a1 = reinterpret_cast<const double2*>(a)[1],
+                a2 = reinterpret_cast<const double2*>(a)[2];
+  const double2 x0 = reinterpret_cast<const double2*>(x)[0], x1 = reinterpret_cast<const double2*>(x)[1],
+                x2 = reinterpret_cast<const double2*>(x)[2];
+  double s0 = a0.x * x0.x, s1 = a0.y * x0.y;
+  s0 = fma(a1.x, x1.x, s0);
+  s1 = fma(a1.y, x1.y, s1);
+  s0 = fma(a2.x, x2.x, s0);
+  s1 = fma(a2.y, x2.y, s1);
+  return s0 + s1;
+}
+__device__ __forceinline__ double dot6(const float* a, const double* x) {
+  const float2 a0 = reinterpret_cast<const float2*>(a)[0], a1 = reinterpret_cast<const float2*>(a)[1],
+               a2 = reinterpret_cast<const float2*>(a)[2];
+  const double2 x0 = reinterpret_cast<const double2*>(x)[0], x1 = reinterpret_cast<const double2*>(x)[1],
+                x2 = reinterpret_cast<const double2*>(x)[2];
+  double s0 = (double)a0.x * x0.x, s1 = (double)a0.y * x0.y;
+  s0 = fma((double)a1.x, x1.x, s0);
+  s1 = fma((double)a1.y, x1.y, s1);
+  s0 = fma((double)a2.x, x2.x, s0);
+  s1 = fma((double)a2.y, x2.y, s1);
+  return s0 + s1;
 }
 
 template <class VT, bool UPPER>
@@ -365,9 +402,11 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
   const int g = lane / 6, r = lane % 6;
   const ProbDev& d = P[p];
   const TriDesc T = UPPER ? d.U : d.L;
-  double* xs = reinterpret_cast<double*>(smem + (size_t)kStages * T.stage);  // capb x 6
-  double* rs = xs + 6 * (size_t)T.capb;                                      // capr x 6
-  double* ring = rs + 6 * (size_t)T.capr;                                    // 2 x capr x 6
+  // xbuf[h]: gathered x (capb x 6) then right-hand sides (capr x 6) of the
+  // chunks with parity h
+  double* xbuf = reinterpret_cast<double*>(smem + (size_t)kStages * T.stage);
+  const size_t xstride = 6 * ((size_t)T.capb + T.capr);
+  double* ring = xbuf + 2 * xstride;  // 2 x capr x 6
   const double* rb = rhs + 6 * (size_t)d.off;
   double* ob = out + 6 * (size_t)d.off;
   if (tid == 0) {
@@ -378,53 +417,38 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
   __syncthreads();
   // chunk byte ranges are read one issue ahead so tid 0 never waits on them
   long long lo = 0, hi = 0;
-  if (tid == 0) {
+  const int producer = kSweepThreads - 32;  // lane 0 of the last warp issues every copy
+  if (tid == producer) {
     lo = T.off[0];
     hi = T.off[1];
   }
-  auto issue = [&](int c) {  // tid 0 only; lo/hi hold chunk c's range
+  auto issue = [&](int c) {  // producer only; lo/hi hold chunk c's range
     uint64_t* b = &bar[c % kStages];
     mbar_expect_tx(b, (unsigned)(hi - lo));
     bulk_g2s(smem + (size_t)(c % kStages) * T.stage, T.stream + lo, (unsigned)(hi - lo), b);
     lo = hi;
     if (c + 2 <= T.nch) hi = T.off[c + 2];
   };
-  if (tid == 0)
+  if (tid == producer)
     for (int c = 0; c < kStages - 1 && c < T.nch; c++) issue(c);
   int issued = min(kStages - 1, T.nch);
-  // values waiting to be stored into xs / rs (destination index, -1: none)
-  double vcur[kGather];
-  int dcur[kGather];
-#pragma unroll
-  for (int u = 0; u < kGather; u++) dcur[u] = -1;
   // chunk 0 has no earlier rows: only its right-hand sides
   if (!mbar_wait(&bar[0], 0u)) abort_flag = 1;
   __syncthreads();
   if (!abort_flag) {
     const int nr0 = reinterpret_cast<const int4*>(smem)->x;
     const int4* ri0 = reinterpret_cast<const int4*>(smem + 32);
-#pragma unroll
-    for (int u = 0; u < kGather; u++) {
-      const int t = tid + u * kSweepThreads;
-      if (t < 6 * nr0) {
-        vcur[u] = rb[6 * (size_t)ri0[t / 6].x + t % 6];
-        dcur[u] = 6 * T.capb + t;
-      }
-    }
+    for (int t = tid; t < 6 * nr0; t += kSweepThreads)
+      cp_async8(xbuf + 6 * T.capb + t, rb + 6 * (size_t)ri0[t / 6].x + t % 6);
+    cp_async_commit();
   }
   int c = 0;
   for (; c < T.nch; c++) {
     const int s = c % kStages;
     if (c > 0 && !mbar_wait(&bar[s], (unsigned)((c / kStages) & 1))) abort_flag = 1;
-    __syncthreads();  // chunk c-1 solved; its stage is free again
+    cp_async_wait_all();  // this thread's copies for chunk c have landed
+    __syncthreads();      // chunk c-1 solved; its stage and xbuf[(c+1)&1] are free
     if (abort_flag) break;
-    if (issued < T.nch) {
-      if (tid == 0) {
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        issue(issued);
-      }
-      issued++;
-    }
     const unsigned char* st = smem + (size_t)s * T.stage;
     const int4 h0 = reinterpret_cast<const int4*>(st)[0];
     const int4 h1 = reinterpret_cast<const int4*>(st)[1];
@@ -436,28 +460,24 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
     const size_t voff = (32 + 16 * (size_t)nr + 8 * (size_t)(nn + nf1) + 4 * (size_t)nr1 + 15) &
                         ~(size_t)15;
     const VT* sv = reinterpret_cast<const VT*>(st + voff);
-    // loads for chunk c+1: far x entries (rows solved by chunks <= c-1, all
-    // complete at the barrier above) and right-hand sides
-    double vnxt[kGather];
-    int dnxt[kGather];
-#pragma unroll
-    for (int u = 0; u < kGather; u++) {
-      const int t = tid + u * kSweepThreads;
-      dnxt[u] = -1;
-      if (t < 6 * nf1) {
-        const int2 f = far1[t / 6];
-        vnxt[u] = ob[6 * (size_t)f.y + t % 6];
-        dnxt[u] = 6 * f.x + t % 6;
-      } else if (t < 6 * (nf1 + nr1)) {
-        const int t2 = t - 6 * nf1;
-        vnxt[u] = rb[6 * (size_t)rows1[t2 / 6] + t2 % 6];
-        dnxt[u] = 6 * T.capb + t2;
+    double* xs = xbuf + xstride * (c & 1);
+    double* rs = xs + 6 * (size_t)T.capb;
+    // asynchronous copies for chunk c+1 (waited for one chunk later): far x
+    // entries (rows solved by chunks <= c-1, complete at the barrier above)
+    // and right-hand sides
+    {
+      double* xn = xbuf + xstride * ((c + 1) & 1);
+      for (int t = tid; t < 6 * (nf1 + nr1); t += kSweepThreads) {
+        if (t < 6 * nf1) {
+          const int2 f = far1[t / 6];
+          cp_async8(xn + 6 * f.x + t % 6, ob + 6 * (size_t)f.y + t % 6);
+        } else {
+          const int t2 = t - 6 * nf1;
+          cp_async8(xn + 6 * T.capb + t2, rb + 6 * (size_t)rows1[t2 / 6] + t2 % 6);
+        }
       }
+      cp_async_commit();
     }
-    // chunk c's far entries and right-hand sides, loaded one chunk ago
-#pragma unroll
-    for (int u = 0; u < kGather; u++)
-      if (dcur[u] >= 0) xs[dcur[u]] = vcur[u];
     // near entries: results of chunk c-1 from the ring
     const double* rp = ring + 6 * (size_t)T.capr * ((c + 1) & 1);
     for (int t = tid; t < 6 * nn; t += kSweepThreads) {
@@ -465,19 +485,30 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
       xs[6 * q.x + t % 6] = rp[6 * q.y + t % 6];
     }
     __syncthreads();
+    // the producer warp (the last) refills the stage chunk c-1 used while
+    // the other warps solve chunk c's rows
+    if (issued < T.nch) {
+      if (tid == producer) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        issue(issued);
+      }
+      issued++;
+    }
     double* wp = ring + 6 * (size_t)T.capr * (c & 1);
-    for (int k = warp; k < nr; k += nw) {
+    for (int k = warp; k < nr && warp < nw - 1; k += nw - 1) {
       const int4 row = ri[k];
       const int i = row.x, rbeg = row.y, rcnt = row.z;
       const int first = UPPER ? 1 : 0;  // U rows start with U_ii^{-1}
       double acc = 0.0;
       if (g < 4) {
-        for (int j = first + g; j < rcnt; j += 4) {
-          const VT* a = sv + (size_t)(rbeg + j) * 36 + 6 * r;
-          const double* xk = xs + 6 * (rbeg + j);
-#pragma unroll
-          for (int cc = 0; cc < 6; cc++) acc = fma((double)a[cc], xk[cc], acc);
+        double acc1 = 0.0;
+        int j = first + g;
+        for (; j + 4 < rcnt; j += 8) {
+          acc += dot6(sv + (size_t)(rbeg + j) * 36 + 6 * r, xs + 6 * (rbeg + j));
+          acc1 += dot6(sv + (size_t)(rbeg + j + 4) * 36 + 6 * r, xs + 6 * (rbeg + j + 4));
         }
+        if (j < rcnt) acc += dot6(sv + (size_t)(rbeg + j) * 36 + 6 * r, xs + 6 * (rbeg + j));
+        acc += acc1;
       }
       acc += __shfl_down_sync(0xffffffffu, acc, 12);
       acc += __shfl_down_sync(0xffffffffu, acc, 6);
@@ -497,14 +528,10 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
         wp[6 * k + lane] = v;
       }
     }
-#pragma unroll
-    for (int u = 0; u < kGather; u++) {
-      vcur[u] = vnxt[u];
-      dcur[u] = dnxt[u];
-    }
   }
+  cp_async_wait_all();  // no copy may land after the kernel ends
   if (!abort_flag && tid == 0 && bytes_ctr) atomicAdd(bytes_ctr, (unsigned long long)T.abytes);
-  if (abort_flag && tid == 0) {
+  if (abort_flag && tid == producer) {
     atomicOr(&ctl->status, ST_TIMEOUT);
     // chunks c .. issued-1 may still be in flight: let them land (bounded)
     for (int q = c; q < issued; q++) mbar_wait(&bar[q % kStages], (unsigned)((q / kStages) & 1));
@@ -801,7 +828,7 @@ static cudaError_t build_tri(gf_precond* p, const std::vector<int32_t>& diag, bo
   }
   int maxc = 0;
   for (int i = 0; i < n; i++) maxc = std::max(maxc, cnt(i));
-  const int capb = std::max(p->prec == GF_PREC_FP32 ? 256 : 128, (maxc + 3) & ~3);
+  const int capb = std::max(p->prec == GF_PREC_FP32 ? 224 : 112, (maxc + 3) & ~3);
   const int capr = 128;
   // pass 1: chunk boundaries (row ranges of `rows`) and block counts
   std::vector<int32_t> ck{0}, cb;  // chunk row starts, padded block counts
@@ -1587,8 +1614,7 @@ gf_status gf_precond_create(gf_assembler* a, int32_t fill_level, int32_t precisi
   if (e == cudaSuccess) e = build_tri(p, diag, false);
   if (e == cudaSuccess) e = build_tri(p, diag, true);
   auto fits = [&](int w) {
-    const gf_precond::Tri& t = p->tri[w];
-    return sweep_smem(p, w) <= kSweepSmemMax && 6 * (t.capb + t.capr) <= kGather * kSweepThreads;
+    return sweep_smem(p, w) <= kSweepSmemMax;
   };
   if (e == cudaSuccess && !(fits(0) && fits(1))) {
     delete p;
