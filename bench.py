@@ -133,6 +133,24 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def job_ms(ms, ws, device):
+    """Per-step time of the whole job: the maximum over ranks of each rank's
+    device-timed step (every rank runs its own replica of the batch)."""
+    if ws == 1:
+        return ms
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(problems_per_rank, ws, ms):
+    """Solves per second of the whole job: every rank's problems over the
+    slowest rank's step time."""
+    return ws * problems_per_rank / (ms / 1e3)
+
+
 def _dist():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -140,19 +158,51 @@ def _dist():
     return ws, rank, local
 
 
-def cpu_baseline_run(problems, fills, budget_s=25.0, threads=None):
+def systematic_sample(meshes, offset, k=4):
+    """Indices of k problems spread evenly over the size ranking (ranks
+    offset, offset + n/k, ...): solves/s over such a sample estimates the
+    whole batch's solves/s without running every large problem on the CPU."""
+    order = sorted(range(len(meshes)), key=lambda i: meshes[i].num_elements)
+    stride = max(len(order) // k, 1)
+    return [order[(offset % stride) + j * stride] for j in range(k) if (offset % stride) + j * stride < len(order)]
+
+
+def cpu_ordering(mesh, fill=8):
+    """The GPU path's ordering rule on the oracle: natural or RCM, whichever
+    gives fewer ILU(fill) levels x blocks per row."""
+    import numpy as np
+
+    from oracle import pyoracle as po
+    rowp0, cols0 = po.bsr_pattern(mesh.conn, mesh.num_nodes)
+    best = None
+    for name, perm in (("natural", np.arange(mesh.num_nodes, dtype=np.int32)),
+                       ("rcm", po.rcm(rowp0, cols0, 0, 1))):
+        rowp, cols = po.permute_pattern(rowp0, cols0, perm)
+        rk, ck = po.iluk_pattern(rowp, cols, fill)
+        nl, _ = po.levels(rk, ck, True)
+        nu, _ = po.levels(rk, ck, False)
+        score = (nl + nu) * len(ck) / mesh.num_nodes
+        if best is None or score < best[0]:
+            best = (score, name)
+    return best[1]
+
+
+def cpu_baseline_run(problems, fills, budget_s=25.0, threads=None, orders=None):
     """Oracle (restated reference CPU path): assembly (OpenMP over elements),
-    FP64 block ILU(k), left-preconditioned GMRES; on as many of the given
-    problems as fit in about budget_s. Returns (solves/s, n, seconds, cores)."""
+    FP64 block ILU(k), right-preconditioned GMRES, in the same ordering and
+    fill as the GPU path; on as many of the given problems as fit in about
+    budget_s. Returns (solves/s, n, seconds, cores)."""
     import numpy as np
 
     from oracle import pyoracle as po
     threads = threads or os.cpu_count() or 1
+    orders = orders or ["rcm"] * len(problems)
     t_total, n = 0.0, 0
-    for m, k in zip(problems, fills):
+    for m, k, o in zip(problems, fills, orders):
         t0 = time.perf_counter()
         rowp0, cols0 = po.bsr_pattern(m.conn, m.num_nodes)
-        perm = po.rcm(rowp0, cols0, 0, 1)
+        perm = (po.rcm(rowp0, cols0, 0, 1) if o == "rcm"
+                else np.arange(m.num_nodes, dtype=np.int32))
         rowp, cols, A, _, perm = po.assemble_jacobian(m, perm=perm, nthreads=threads)
         po.apply_bcs_mat(rowp, cols, A, perm, m.bcs)
         b = np.zeros(6 * m.num_nodes)
@@ -222,12 +272,13 @@ def run_reference(args):
     if rank != 0:
         return
     probs = M.batch_config4(args.problems)
-    order = sorted(range(len(probs)), key=lambda i: probs[i].num_elements)
-    sample = [probs[i] for i in order]
-    fills = [_default_fill(p) for p in sample]
     vals = []
     for s in range(args.warmup + args.steps):
-        v, n, sec, cores = cpu_baseline_run(sample, fills, budget_s=20.0)
+        idx = systematic_sample(probs, 2 + 5 * s)
+        sample = [probs[i] for i in idx]
+        v, n, sec, cores = cpu_baseline_run(sample, [_default_fill(p) for p in sample],
+                                            budget_s=1e9,
+                                            orders=[cpu_ordering(p) for p in sample])
         if s >= args.warmup:
             vals.append(v)
     value = statistics.median(vals)
@@ -235,9 +286,12 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * n / value,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (seeded meshes)", "impl": "reference",
-            "config": {"workload": WORKLOAD, "sample": f"{n} smallest problems per step"},
+            "config": {"workload": WORKLOAD,
+                       "sample": "4 problems per step spread over the size ranking"},
             "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port",
-                             "sample": f"{n} smallest of the 64 problems, ~20 s per step"},
+                             "sample": "per step 4 of the 64 problems at size ranks o, o+16, "
+                                       "o+32, o+48 (o varies by step); ILU(8), same "
+                                       "ordering rule as the GPU path"},
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -315,12 +369,7 @@ def main():
             L.check(L.lib().gf_timing_enable(0), "timing")
             timed.sweep = (sm.value, sl.value, sb.value)
         lat = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
-        ms = ev[0].elapsed_time(ev[-1]) / args.steps
-        if ws > 1:
-            import torch.distributed as dist
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = job_ms(ev[0].elapsed_time(ev[-1]) / args.steps, ws, "cuda")
         timed.iters = its
         return ms, lat
 
@@ -340,7 +389,7 @@ def main():
     ms_e2e, _ = timed(True, (host_b, host_x))
     h2d = sum(8 * m.num_dof for m in meshes)
     nprob = len(meshes)
-    value = ws * nprob / (ms_mixed / 1e3)
+    value = job_throughput(nprob, ws, ms_mixed)
 
     # roofline of the dominant kernel, the block triangular sweeps
     # (bsweep_tma), from CUDA events around every sweep pair inside the timed
@@ -363,14 +412,14 @@ def main():
         "latency_ms": {"p50": float(np.percentile(lat_mixed, 50)),
                        "p99": float(np.percentile(lat_mixed, 99)),
                        "note": "all 64 requests of a step complete together"},
-        "fp64_gpu": {"value": ws * nprob / (ms_fp64 / 1e3), "unit": "solves/s",
+        "fp64_gpu": {"value": job_throughput(nprob, ws, ms_fp64), "unit": "solves/s",
                      "ms_per_step": ms_fp64,
                      "latency_ms": {"p50": float(np.percentile(lat_fp64, 50)),
                                     "p99": float(np.percentile(lat_fp64, 99))}},
         "mixed_over_fp64": ms_fp64 / ms_mixed,
         "phase_ms": {"assemble": phases_mixed[0], "factor": phases_mixed[1],
                      "solve": phases_mixed[2]},
-        "e2e": {"value": ws * nprob / (ms_e2e / 1e3), "unit": "solves/s",
+        "e2e": {"value": job_throughput(nprob, ws, ms_e2e), "unit": "solves/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
         "roofline": {"kernel": "bsweep_tma (block L and U sweeps, FP32 factor values)",
                      "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -383,12 +432,13 @@ def main():
         "gpu_launches": int(launches),
     }
     if rank == 0 and not args.no_cpu_baseline and ws == 1:
-        order = sorted(range(nprob), key=lambda i: meshes[i].num_elements)
-        v, n_cpu, sec, cores = cpu_baseline_run([meshes[i] for i in order],
-                                                [bs.fills[i] for i in order],
-                                                budget_s=20.0)
+        idx = systematic_sample(meshes, 2)
+        v, n_cpu, sec, cores = cpu_baseline_run([meshes[i] for i in idx],
+                                                [bs.fills[i] for i in idx], budget_s=1e9,
+                                                orders=[bs.orderings[i] for i in idx])
         line["cpu_baseline"] = {"value": v, "unit": "solves/s", "cores": cores, "kind": "port",
-                                "sample": f"{n_cpu} smallest of the 64 problems ({sec:.1f} s)"}
+                                "sample": f"{n_cpu} of the 64 problems at size ranks 2, 18, 34, "
+                                          f"50, same fill and ordering as the GPU ({sec:.1f} s)"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if ws > 1:
