@@ -15,8 +15,7 @@ symbolic ILU(k) (computeILUk, include/linalg/bsr_utils.h:678-807) is chosen
 per problem: every candidate k is tried on the whole batch in one batched
 solve (FP32 factors, the less forgiving precision, inside FP64 GMRES) with
 an iteration cap, and each problem keeps the converging k
-with the smallest estimated critical path (iterations x triangular levels
-for the sweeps, lower levels x lower blocks per row for the factorization).
+with the smallest modelled factor + solve time (step_cost_us).
 The node ordering (natural or RCM) is chosen first, by levels x blocks per
 row of ILU(8).
 """
@@ -79,6 +78,22 @@ def solve_opts(rtol=1e-8, mixed=False, restart=100, max_iters=20000, inner_rtol=
 
 
 ORDERINGS = ("natural", "rcm")
+
+
+def step_cost_us(nrow, inf, iterations):
+    """Critical-path model of one factor + solve of a problem (microseconds),
+    fitted to B200 runs of the 64-plate batch. The factorization walks its
+    lower levels in rounds of 16 rows (one per warp); a row's steps are
+    sequential and each updates about one row length of blocks, so a row
+    costs ~0.35 us x (lower blocks)^2. Every GMRES step runs both sweeps at
+    ~1.1 us a level plus ~9 ns per block of the level, and ~30 us of SpMV and
+    reductions."""
+    lvl, lvu, nnzb = inf["levels_L"], inf["levels_U"], inf["nnzb"]
+    lower = max(nnzb - nrow, 0) / (2.0 * nrow)
+    rounds = -(-nrow // max(lvl, 1) // 16) or 1
+    factor = lvl * rounds * 0.35 * lower * lower
+    per_level = 1.1 + 0.009 * max(nnzb - nrow, 0) / 2.0 / max(lvl, 1)
+    return factor + iterations * ((lvl + lvu) * per_level + 30.0)
 
 
 def choose_ordering(mesh, fill=8):
@@ -170,12 +185,7 @@ class BatchSolver:
                 ok = s["status"] == L.GF_OK
                 log.append((i, k, s["iterations"], s["rel_residual"], nlev, ok))
                 if ok:
-                    # critical-path model (microseconds): every iteration runs
-                    # both sweeps (~2 us a level); the factorization takes
-                    # ~1 us per lower block of a row along the lower levels
-                    nrow = self.asms[i].get_num_nodes()
-                    lower = max(inf["nnzb"] - nrow, 0) / (2.0 * nrow)
-                    cost = 2.0 * s["iterations"] * nlev + inf["levels_L"] * lower
+                    cost = step_cost_us(self.asms[i].get_num_nodes(), inf, s["iterations"])
                     if best[i] is None or cost < best[i][0]:
                         best[i] = (cost, k, k)
             if all(b is not None for b in best) and k >= max(b[1] for b in best) + 4:
