@@ -293,7 +293,7 @@ __global__ void convert_kernel(size_t n, const double* __restrict__ in, T2* __re
 // its rows' 6x6 products. x / y live in global memory, written and re-read
 // by this CTA only.
 constexpr int kSweepThreads = 512;
-constexpr int kStages = 4;
+constexpr int kStages = 3;
 constexpr unsigned long long kWaitNs = 2000000000ull;
 constexpr size_t kSweepSmemMax = 220 * 1024;  // dynamic; the static part is < 1 KB
 
@@ -351,6 +351,10 @@ __host__ __device__ inline size_t sweep_smem_bytes(int stage, int capb, int capr
 }
 __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src)
                : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() {
@@ -435,11 +439,20 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
   // chunk 0 has no earlier rows: only its right-hand sides
   if (!mbar_wait(&bar[0], 0u)) abort_flag = 1;
   __syncthreads();
+  // 6-double rows of x and of the right-hand side move as three 16-byte
+  // pieces when both vectors are 16-byte aligned, else as six 8-byte ones
+  const int pw = ((reinterpret_cast<uintptr_t>(rb) | reinterpret_cast<uintptr_t>(ob)) & 15) ? 6 : 3;
+  auto copy_piece = [&](double* dst, const double* src, int piece) {
+    if (pw == 3)
+      cp_async16(dst + 2 * piece, src + 2 * piece);
+    else
+      cp_async8(dst + piece, src + piece);
+  };
   if (!abort_flag) {
     const int nr0 = reinterpret_cast<const int4*>(smem)->x;
     const int4* ri0 = reinterpret_cast<const int4*>(smem + 32);
-    for (int t = tid; t < 6 * nr0; t += kSweepThreads)
-      cp_async8(xbuf + 6 * T.capb + t, rb + 6 * (size_t)ri0[t / 6].x + t % 6);
+    for (int t = tid; t < pw * nr0; t += kSweepThreads)
+      copy_piece(xbuf + 6 * T.capb + 6 * (t / pw), rb + 6 * (size_t)ri0[t / pw].x, t % pw);
     cp_async_commit();
   }
   int c = 0;
@@ -467,22 +480,26 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
     // and right-hand sides
     {
       double* xn = xbuf + xstride * ((c + 1) & 1);
-      for (int t = tid; t < 6 * (nf1 + nr1); t += kSweepThreads) {
-        if (t < 6 * nf1) {
-          const int2 f = far1[t / 6];
-          cp_async8(xn + 6 * f.x + t % 6, ob + 6 * (size_t)f.y + t % 6);
+      for (int t = tid; t < pw * (nf1 + nr1); t += kSweepThreads) {
+        if (t < pw * nf1) {
+          const int2 f = far1[t / pw];
+          copy_piece(xn + 6 * f.x, ob + 6 * (size_t)f.y, t % pw);
         } else {
-          const int t2 = t - 6 * nf1;
-          cp_async8(xn + 6 * T.capb + t2, rb + 6 * (size_t)rows1[t2 / 6] + t2 % 6);
+          const int t2 = t - pw * nf1;
+          copy_piece(xn + 6 * T.capb + 6 * (t2 / pw), rb + 6 * (size_t)rows1[t2 / pw], t2 % pw);
         }
       }
       cp_async_commit();
     }
     // near entries: results of chunk c-1 from the ring
-    const double* rp = ring + 6 * (size_t)T.capr * ((c + 1) & 1);
-    for (int t = tid; t < 6 * nn; t += kSweepThreads) {
-      const int2 q = nearl[t / 6];
-      xs[6 * q.x + t % 6] = rp[6 * q.y + t % 6];
+    {
+      const double2* rp =
+          reinterpret_cast<const double2*>(ring + 6 * (size_t)T.capr * ((c + 1) & 1));
+      double2* xs2 = reinterpret_cast<double2*>(xs);
+      for (int t = tid; t < 3 * nn; t += kSweepThreads) {
+        const int2 q = nearl[t / 3];
+        xs2[3 * q.x + t % 3] = rp[3 * q.y + t % 3];
+      }
     }
     __syncthreads();
     // the producer warp (the last) refills the stage chunk c-1 used while
@@ -828,7 +845,7 @@ static cudaError_t build_tri(gf_precond* p, const std::vector<int32_t>& diag, bo
   }
   int maxc = 0;
   for (int i = 0; i < n; i++) maxc = std::max(maxc, cnt(i));
-  const int capb = std::max(p->prec == GF_PREC_FP32 ? 224 : 112, (maxc + 3) & ~3);
+  const int capb = std::max(p->prec == GF_PREC_FP32 ? 320 : 160, (maxc + 3) & ~3);
   const int capr = 128;
   // pass 1: chunk boundaries (row ranges of `rows`) and block counts
   std::vector<int32_t> ck{0}, cb;  // chunk row starts, padded block counts

@@ -148,3 +148,28 @@ def test_mixed_precision_refinement_reaches_fp64_tolerance(oracle):
         assert stats["rel_residual"] <= 1e-8, (mixed, stats)
         err = np.linalg.norm(x.cpu().numpy() - x_dense) / np.linalg.norm(x_dense)
         assert err <= 1e-6, (mixed, err, stats)
+
+
+def test_precond_apply_accepts_8_byte_aligned_vectors():
+    """The sweeps move 6-double rows as 16-byte pieces when the vectors allow
+    and as 8-byte pieces otherwise; both give the same z bit for bit."""
+    import torch
+    from gpu_fem_b200.assembler import ILUk_Preconditioner
+    mesh = M.plate_config2(24, 12)
+    from gpu_fem_b200.assembler import ElementAssembler, createBsrMat
+    A = ElementAssembler.from_mesh(mesh, ordering="rcm")
+    K = createBsrMat(A)
+    A.add_jacobian(None, K, fuse_bcs=True)
+    for prec in ("fp64", "fp32"):
+        P = ILUk_Preconditioner(A, fill_level=2, precision=prec)
+        P.factor(K)
+        n = mesh.num_dof
+        r = torch.tensor(np.random.default_rng(5).standard_normal(n), device="cuda")
+        z = torch.zeros_like(r)
+        P.apply(r, z)
+        rb = torch.zeros(n + 1, dtype=torch.float64, device="cuda")
+        zb = torch.zeros(n + 1, dtype=torch.float64, device="cuda")
+        rb[1:] = r
+        P.apply(rb[1:], zb[1:])  # both vectors 8 bytes off a 16-byte boundary
+        torch.cuda.synchronize()
+        assert np.array_equal(z.cpu().numpy().view(np.uint64), zb[1:].cpu().numpy().view(np.uint64))
