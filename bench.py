@@ -44,10 +44,59 @@ def _args():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--problems", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-seconds", type=float, default=0.0,
+                    help="length of the Poisson request stream of the serving run (0 skips it)")
+    ap.add_argument("--assembly-case", action="store_true",
+                    help="small profiling case: Jacobian assembly (fused BCs) of the 400x200 "
+                         "jittered cantilever plate, 5 times (no JSON line)")
     ap.add_argument("--sweep-case", action="store_true",
                     help="small profiling case: the triangular sweeps of one 256x128 plate, "
                          "ILU(6), FP32 factors, applied 5 times (no JSON line)")
     return ap.parse_args()
+
+
+SERVE_RATE, SERVE_MAX_CLASS = 20.0, 8
+
+
+def serving_run(seconds):
+    """Continuous-batching server on a Poisson stream of plate and box
+    requests (rate 20/s, size classes 5e3..1.2e5 DOF, per-request thickness
+    field and load from the request seed), once with FP32 ILU factors
+    (mixed) and once with FP64 factors, each to a 1e-8 relative residual.
+    Size classes are built and their fill tuned before the stream starts."""
+    from gpu_fem_b200 import serve
+    out, fills, n = {}, None, 0
+    for prec, name in (("fp32", "mixed"), ("fp64", "fp64")):
+        reqs = serve.poisson_requests(rate=SERVE_RATE, duration=seconds, seed=99,
+                                      max_class=SERVE_MAX_CLASS)
+        n = len(reqs)
+        srv = serve.Server(budget_gb=40.0, streams=4, max_batch=16, precision=prec, fills=fills)
+        srv.warm({(r.family, r.cls) for r in reqs})
+        fills = dict(srv.fills)
+        res = srv.run(reqs)
+        out[name] = {k: res[k] for k in ("requests", "solved", "solves_per_s", "p50_ms", "p99_ms",
+                                          "wall_s")}
+    out["stream"] = (f"Poisson {SERVE_RATE:g} req/s for {seconds:g} s, {n} requests, plates and "
+                     f"stiffened boxes, size classes 0..{SERVE_MAX_CLASS} (5e3..1.2e5 DOF); "
+                     f"latency = completion - arrival")
+    return out
+
+
+def assembly_case():
+    """Jacobian assembly with fused BCs of the 400x200 plate (80,601 nodes,
+    ~209 MB of block values, above L2), 5 times: the small case on which the
+    assembly kernel is profiled."""
+    import torch
+    from gpu_fem_b200 import mesh as M
+    from gpu_fem_b200.assembler import ElementAssembler, createBsrMat
+    m = M.plate_config2()
+    A = ElementAssembler.from_mesh(m, ordering="rcm")
+    K = createBsrMat(A)
+    res = A.createVarsVec()
+    for _ in range(5):
+        A.add_jacobian(res, K, fuse_bcs=True)
+    torch.cuda.synchronize()
+    print("assembly case", A.get_nnzb())
 
 
 def sweep_case():
@@ -306,6 +355,8 @@ def main():
     args = _args()
     if args.sweep_case:
         return sweep_case()
+    if args.assembly_case:
+        return assembly_case()
     if args.impl == "reference":
         return run_reference(args)
     import numpy as np
@@ -431,6 +482,8 @@ def main():
         "clocks": clk,
         "gpu_launches": int(launches),
     }
+    if args.serve_seconds > 0:
+        line["serving"] = serving_run(args.serve_seconds)
     if rank == 0 and not args.no_cpu_baseline and ws == 1:
         idx = systematic_sample(meshes, 2)
         v, n_cpu, sec, cores = cpu_baseline_run([meshes[i] for i in idx],

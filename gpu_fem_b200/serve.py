@@ -99,11 +99,12 @@ def poisson_requests(rate, duration, seed=99, nclasses=16, families=("plate", "b
 
 
 class SizeClass:
-    def __init__(self, family, k, dof, fill=None, rtol=1e-8):
+    def __init__(self, family, k, dof, fill=None, rtol=1e-8, precision="fp32"):
         self.family, self.k = family, k
         self.mesh = class_mesh(family, dof)
         self.ordering, self.asm = choose_ordering(self.mesh)
         self.fill = fill if fill is not None else tune_class_fill(self.mesh, self.ordering, rtol)
+        self.precision = precision
         self.free = []
         self.lock = threading.Lock()
         nn, ne = self.mesh.num_nodes, self.mesh.num_elements
@@ -114,7 +115,7 @@ class SizeClass:
 
     def make_slot(self):
         K = BsrMat(self.asm)
-        P = ILUk_Preconditioner(self.asm, self.fill, "fp32")
+        P = ILUk_Preconditioner(self.asm, self.fill, self.precision)
         n = self.mesh.num_dof
         return {"K": K, "P": P, "b": torch.zeros(n, dtype=torch.float64, device="cuda"),
                 "x": torch.zeros(n, dtype=torch.float64, device="cuda"),
@@ -135,12 +136,13 @@ class SizeClass:
 
 class Server:
     def __init__(self, budget_gb=120.0, streams=4, max_batch=64, classes=None, restart=100,
-                 rtol=1e-8, fills=None, max_iters=3000):
+                 rtol=1e-8, fills=None, max_iters=3000, precision="fp32"):
         self.budget = budget_gb * 1e9
         self.used = 0.0
         self.mem_lock = threading.Lock()
         self.max_batch = max_batch
         self.restart, self.rtol, self.max_iters = restart, rtol, max_iters
+        self.precision = precision  # ILU factor values: "fp32" (mixed) or "fp64"
         self.classes = {}
         self.streams = [torch.cuda.Stream() for _ in range(streams)]
         self.work = queue.Queue()
@@ -156,7 +158,8 @@ class Server:
         key = (family, k)
         if key not in self.classes:
             dof = size_classes()[k]
-            self.classes[key] = SizeClass(family, k, dof, self.fills.get(key), self.rtol)
+            self.classes[key] = SizeClass(family, k, dof, self.fills.get(key), self.rtol,
+                                          self.precision)
             self.fills[key] = self.classes[key].fill
         return self.classes[key]
 
