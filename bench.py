@@ -55,12 +55,12 @@ def _args():
     return ap.parse_args()
 
 
-SERVE_RATE, SERVE_MAX_CLASS = 20.0, 8
+SERVE_RATE, SERVE_MAX_CLASS = 20.0, 6
 
 
 def serving_run(seconds):
     """Continuous-batching server on a Poisson stream of plate and box
-    requests (rate 20/s, size classes 5e3..1.2e5 DOF, per-request thickness
+    requests (rate 20/s, size classes 5e3..5.5e4 DOF, per-request thickness
     field and load from the request seed), once with FP32 ILU factors
     (mixed) and once with FP64 factors, each to a 1e-8 relative residual.
     Size classes are built and their fill tuned before the stream starts."""
@@ -77,7 +77,7 @@ def serving_run(seconds):
         out[name] = {k: res[k] for k in ("requests", "solved", "solves_per_s", "p50_ms", "p99_ms",
                                           "wall_s")}
     out["stream"] = (f"Poisson {SERVE_RATE:g} req/s for {seconds:g} s, {n} requests, plates and "
-                     f"stiffened boxes, size classes 0..{SERVE_MAX_CLASS} (5e3..1.2e5 DOF); "
+                     f"stiffened boxes, size classes 0..{SERVE_MAX_CLASS} (5e3..5.5e4 DOF); "
                      f"latency = completion - arrival")
     return out
 

@@ -81,8 +81,10 @@ def poisson_requests(rate, duration, seed=99, nclasses=16, families=("plate", "b
                      max_class=None):
     g = M.MT19937_64(seed)
     reqs, t, rid = [], 0.0, 0
-    lo, hi = math.log(5e3), math.log(2e6)
     classes = size_classes(nclasses)
+    # sizes log-uniform over 5e3..2e6 DOF, or up to the largest allowed class
+    lo = math.log(5e3)
+    hi = math.log(2e6 if max_class is None else classes[max_class])
     while True:
         u = g.uniform(4)
         t += -math.log(max(u[0], 1e-300)) / rate
@@ -91,8 +93,6 @@ def poisson_requests(rate, duration, seed=99, nclasses=16, families=("plate", "b
         fam = families[int(u[1] * len(families)) % len(families)]
         dof = math.exp(lo + u[2] * (hi - lo))
         cls = int(np.argmin([abs(math.log(dof / c)) for c in classes]))
-        if max_class is not None:
-            cls = min(cls, max_class)
         reqs.append(Request(rid, t, fam, cls, int(u[3] * 2 ** 31)))
         rid += 1
     return reqs
@@ -243,11 +243,13 @@ class Server:
                 requests[i].t0 = t_start + requests[i].arrival * time_scale
                 pending.append(requests[i])
                 i += 1
-            # admit FIFO while slots and memory allow, batch per dispatch
-            batch = []
+            # admit FIFO while slots and memory allow; one batch per size class
+            # (requests of a class cost alike, so none waits on a slower kind)
+            groups = {}
             keep = []
             for req in pending:
                 cls = self.get_class(req.family, req.cls)
+                batch = groups.setdefault((req.family, req.cls), [])
                 ok = len(batch) < self.max_batch
                 if ok:
                     with self.mem_lock:
@@ -263,13 +265,16 @@ class Server:
                     slot = cls.make_slot()
                 batch.append((req, cls, slot))
             pending = keep
-            if batch:
-                self.work.put(batch)
+            dispatched = False
+            for batch in groups.values():
+                if batch:
+                    self.work.put(batch)
+                    dispatched = True
             with self.done_lock:
                 ndone = len(self.completed)
             if i >= nreq and not pending and ndone >= nreq:
                 break
-            if not batch:
+            if not dispatched:
                 time.sleep(0.002)
         for _ in threads:
             self.work.put(None)
