@@ -28,6 +28,7 @@
 #include <cstring>
 #include <mutex>
 #include <numeric>
+#include <type_traits>
 
 #include "gf_internal.h"
 
@@ -441,9 +442,17 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
   __syncthreads();
   // 6-double rows of x and of the right-hand side move as three 16-byte
   // pieces when both vectors are 16-byte aligned, else as six 8-byte ones
-  const int pw = ((reinterpret_cast<uintptr_t>(rb) | reinterpret_cast<uintptr_t>(ob)) & 15) ? 6 : 3;
-  auto copy_piece = [&](double* dst, const double* src, int piece) {
-    if (pw == 3)
+  const bool a16 = ((reinterpret_cast<uintptr_t>(rb) | reinterpret_cast<uintptr_t>(ob)) & 15) == 0;
+  // pieces per row as a compile-time constant (3 or 6): the index splits
+  // below then compile to multiplications instead of divisions
+  auto with_pw = [&](auto fn) {
+    if (a16)
+      fn(std::integral_constant<int, 3>{});
+    else
+      fn(std::integral_constant<int, 6>{});
+  };
+  auto copy_piece = [](auto pwc, double* dst, const double* src, int piece) {
+    if (decltype(pwc)::value == 3)
       cp_async16(dst + 2 * piece, src + 2 * piece);
     else
       cp_async8(dst + piece, src + piece);
@@ -451,8 +460,11 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
   if (!abort_flag) {
     const int nr0 = reinterpret_cast<const int4*>(smem)->x;
     const int4* ri0 = reinterpret_cast<const int4*>(smem + 32);
-    for (int t = tid; t < pw * nr0; t += kSweepThreads)
-      copy_piece(xbuf + 6 * T.capb + 6 * (t / pw), rb + 6 * (size_t)ri0[t / pw].x, t % pw);
+    with_pw([&](auto pwc) {
+      constexpr int pw = decltype(pwc)::value;
+      for (int t = tid; t < pw * nr0; t += kSweepThreads)
+        copy_piece(pwc, xbuf + 6 * T.capb + 6 * (t / pw), rb + 6 * (size_t)ri0[t / pw].x, t % pw);
+    });
     cp_async_commit();
   }
   int c = 0;
@@ -480,15 +492,19 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
     // and right-hand sides
     {
       double* xn = xbuf + xstride * ((c + 1) & 1);
-      for (int t = tid; t < pw * (nf1 + nr1); t += kSweepThreads) {
-        if (t < pw * nf1) {
-          const int2 f = far1[t / pw];
-          copy_piece(xn + 6 * f.x, ob + 6 * (size_t)f.y, t % pw);
-        } else {
-          const int t2 = t - pw * nf1;
-          copy_piece(xn + 6 * T.capb + 6 * (t2 / pw), rb + 6 * (size_t)rows1[t2 / pw], t2 % pw);
+      with_pw([&](auto pwc) {
+        constexpr int pw = decltype(pwc)::value;
+        for (int t = tid; t < pw * (nf1 + nr1); t += kSweepThreads) {
+          if (t < pw * nf1) {
+            const int2 f = far1[t / pw];
+            copy_piece(pwc, xn + 6 * f.x, ob + 6 * (size_t)f.y, t % pw);
+          } else {
+            const int t2 = t - pw * nf1;
+            copy_piece(pwc, xn + 6 * T.capb + 6 * (t2 / pw), rb + 6 * (size_t)rows1[t2 / pw],
+                       t2 % pw);
+          }
         }
-      }
+      });
       cp_async_commit();
     }
     // near entries: results of chunk c-1 from the ring
