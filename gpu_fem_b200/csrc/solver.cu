@@ -284,8 +284,8 @@ __global__ void convert_kernel(size_t n, const double* __restrict__ in, T2* __re
 // One CTA per problem walks the chunks of one triangle in level-major order
 // (a chunk holds rows of one level). A ring of kStages shared-memory stages
 // is filled by 1D bulk copies (cp.async.bulk, completion counted on an
-// mbarrier) kStages-1 chunks ahead, so the factor values are never waited
-// for. The x entries a chunk multiplies come from two places:
+// mbarrier) kStages-1 chunks ahead of the chunk being solved. The x
+// entries a chunk multiplies come from two places:
 //  - near: rows solved by the previous chunk, kept in a shared-memory ring;
 //  - far: rows solved two or more chunks earlier, loaded from global memory
 //    one chunk ahead (issued right after the barrier that ends chunk c-1,
@@ -294,7 +294,7 @@ __global__ void convert_kernel(size_t n, const double* __restrict__ in, T2* __re
 // its rows' 6x6 products. x / y live in global memory, written and re-read
 // by this CTA only.
 constexpr int kSweepThreads = 512;
-constexpr int kStages = 3;
+constexpr int kStages = 2;
 constexpr unsigned long long kWaitNs = 2000000000ull;
 constexpr size_t kSweepSmemMax = 220 * 1024;  // dynamic; the static part is < 1 KB
 
@@ -861,7 +861,7 @@ static cudaError_t build_tri(gf_precond* p, const std::vector<int32_t>& diag, bo
   }
   int maxc = 0;
   for (int i = 0; i < n; i++) maxc = std::max(maxc, cnt(i));
-  const int capb = std::max(p->prec == GF_PREC_FP32 ? 320 : 160, (maxc + 3) & ~3);
+  const int capb = std::max(p->prec == GF_PREC_FP32 ? 416 : 208, (maxc + 3) & ~3);
   const int capr = 128;
   // pass 1: chunk boundaries (row ranges of `rows`) and block counts
   std::vector<int32_t> ck{0}, cb;  // chunk row starts, padded block counts
