@@ -473,7 +473,6 @@ inline void sym_rotate_T(const T A[9], const T eb[6], T gb[6]) {
   gb[4] = M[5] + M[7];
   gb[5] = M[8];
 }
-struct QuadGeom;  // fwd
 
 // ShellComputeDispGrad (basis.h:427-502); returns detXd
 template <class T>
@@ -625,7 +624,6 @@ inline void shell_stress(const ShellData& d, const T E[9], T S[9]) {
 }
 
 // ----------------------------------------------- per-quadrature-point ops
-struct Fwd;
 template <class T>
 struct QuadFwd {
   T fn[12], d[12], ety[9], u0x[9], u1x[9], e0ty[6], et, detXd, scale, pt[2];
