@@ -453,7 +453,7 @@ def main():
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_mixed,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64 assembly + f32 ILU/SpMV in f64 GMRES/IR", "data": "synthetic (seeded meshes)",
+        "dtype": "f64 assembly, SpMV and GMRES; f32 ILU factor values", "data": "synthetic (seeded meshes)",
         "config": {"workload": WORKLOAD, "problems": nprob,
                    "dofs": int(sum(m.num_dof for m in meshes)),
                    "fill_levels": bs.fills,
