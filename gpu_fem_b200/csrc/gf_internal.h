@@ -116,9 +116,10 @@ struct TriDesc {
   int nch;                       // chunks
   int stage;                     // bytes of the largest chunk (staging buffer size)
   int capb, capr;                // blocks / rows per chunk at most
-  const int64_t* off;            // [nch+1] byte offsets into stream
+  const int64_t* off;            // [2 (nch+1)] byte offsets of the two halves' chunks
   const unsigned char* stream;
   long long abytes;              // algorithmic bytes of one sweep (for timing)
+  int nsplit;                    // CTAs that share each chunk's rows (1 or 2)
 };
 
 // Per-problem descriptor used by the batched solver kernels: block rows,

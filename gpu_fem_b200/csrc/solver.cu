@@ -281,19 +281,25 @@ __global__ void convert_kernel(size_t n, const double* __restrict__ in, T2* __re
 
 
 // ------------------------------------------- prefetched level-major sweeps
-// One CTA per problem walks the chunks of one triangle in level-major order
-// (a chunk holds rows of one level). A ring of kStages shared-memory stages
+// A thread-block cluster of kSweepCta CTAs per problem walks the chunks of
+// one triangle in level-major order (a chunk holds rows of one level); each
+// CTA solves its half of every chunk's rows from its own stream, and the
+// CTAs meet once per chunk on a pair of mbarriers (bounded waits, release /
+// acquire at cluster scope). A ring of kStages shared-memory stages
 // is filled by 1D bulk copies (cp.async.bulk, completion counted on an
 // mbarrier) kStages-1 chunks ahead of the chunk being solved. The x
 // entries a chunk multiplies come from two places:
-//  - near: rows solved by the previous chunk, kept in a shared-memory ring;
+//  - near: rows solved by the previous chunk, kept in a shared-memory ring
+//    that both CTAs write (their own and, through distributed shared
+//    memory, the partner's);
 //  - far: rows solved two or more chunks earlier, loaded from global memory
 //    one chunk ahead (issued right after the barrier that ends chunk c-1,
 //    consumed by chunk c+1), together with chunk c+1's right-hand sides;
 // so a chunk's critical path is two block barriers, shared-memory copies and
 // its rows' 6x6 products. x / y live in global memory, written and re-read
-// by this CTA only.
+// by the problem's cluster only.
 constexpr int kSweepThreads = 512;
+constexpr int kSweepCta = 2;  // CTAs (one thread-block cluster) per problem and sweep
 constexpr int kStages = 2;
 constexpr unsigned long long kWaitNs = 2000000000ull;
 constexpr size_t kSweepSmemMax = 220 * 1024;  // dynamic; the static part is < 1 KB
@@ -343,12 +349,54 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
       : "memory");
 }
 
+__device__ __forceinline__ unsigned cluster_rank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+// address of the same shared-memory location in CTA `rank` of the cluster
+__device__ __forceinline__ unsigned cluster_map(unsigned addr, unsigned rank) {
+  unsigned r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void cluster_store(unsigned addr, double v) {
+  asm volatile("st.shared::cluster.f64 [%0], %1;" ::"r"(addr), "d"(v) : "memory");
+}
+// arrive on an mbarrier of another CTA of the cluster (releases this CTA's
+// earlier writes at cluster scope)
+__device__ __forceinline__ void mbar_arrive_remote(unsigned addr) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(addr)
+               : "memory");
+}
+// bounded wait with acquire at cluster scope; false if kWaitNs passed first
+__device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, unsigned parity) {
+  const unsigned long long t0 = gtimer();
+  unsigned n = 0;
+  while (true) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if ((++n & 255u) == 0u && gtimer() - t0 > kWaitNs) return false;
+  }
+}
+// all threads of all CTAs of the cluster
+__device__ __forceinline__ void cluster_barrier() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\nbarrier.cluster.wait.acquire.aligned;" :::
+                   "memory");
+}
+
 // Dynamic shared memory of one sweep: kStages staging buffers of `stage`
 // bytes; two buffers (this chunk, next chunk) of gathered x (capb x 6
 // doubles) and right-hand sides (capr x 6); the ring of the two latest
-// chunks' results (2 capr x 6).
+// chunks' results (2 slots x kSweepCta capr rows x 6).
 __host__ __device__ inline size_t sweep_smem_bytes(int stage, int capb, int capr) {
-  return kStages * (size_t)stage + 96 * ((size_t)capb + 2 * (size_t)capr);
+  return kStages * (size_t)stage + 96 * ((size_t)capb + capr) + 96 * (size_t)kSweepCta * capr;
 }
 __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src)
@@ -400,9 +448,13 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
                                                            unsigned long long* bytes_ctr) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint64_t bar[kStages];
+  __shared__ uint64_t xbar[2];  // the partner's "chunk done" arrivals, alternating
   __shared__ int abort_flag;
-  const int p = blockIdx.x;
-  if (live && !live[p]) return;
+  const int p = blockIdx.x / kSweepCta;
+  const unsigned rank = cluster_rank(), partner = rank ^ 1u;
+  if (live && !live[p]) return;  // the same for every CTA of the cluster
+  const bool split = (UPPER ? P[p].U.nsplit : P[p].L.nsplit) > 1;
+  if (!split && rank != 0) return;  // one CTA solves the whole chunk; no cluster traffic
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
   const int g = lane / 6, r = lane % 6;
   const ProbDev& d = P[p];
@@ -411,28 +463,37 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
   // chunks with parity h
   double* xbuf = reinterpret_cast<double*>(smem + (size_t)kStages * T.stage);
   const size_t xstride = 6 * ((size_t)T.capb + T.capr);
-  double* ring = xbuf + 2 * xstride;  // 2 x capr x 6
+  const int ringrows = kSweepCta * T.capr;
+  double* ring = xbuf + 2 * xstride;  // 2 x ringrows x 6
+  const unsigned pring = cluster_map(smem_u32(ring), partner);
+  const unsigned pxbar = cluster_map(smem_u32(xbar), partner);
+  const int64_t* offs = T.off + (size_t)rank * (T.nch + 1);  // this CTA's half chunks
   const double* rb = rhs + 6 * (size_t)d.off;
   double* ob = out + 6 * (size_t)d.off;
   if (tid == 0) {
     for (int s = 0; s < kStages; s++) mbar_init(&bar[s], 1);
+    mbar_init(&xbar[0], 1);
+    mbar_init(&xbar[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     abort_flag = 0;
   }
-  __syncthreads();
+  if (split)
+    cluster_barrier();  // both CTAs' barriers exist before any remote arrival
+  else
+    __syncthreads();
   // chunk byte ranges are read one issue ahead so tid 0 never waits on them
   long long lo = 0, hi = 0;
   const int producer = kSweepThreads - 32;  // lane 0 of the last warp issues every copy
   if (tid == producer) {
-    lo = T.off[0];
-    hi = T.off[1];
+    lo = offs[0];
+    hi = offs[1];
   }
   auto issue = [&](int c) {  // producer only; lo/hi hold chunk c's range
     uint64_t* b = &bar[c % kStages];
     mbar_expect_tx(b, (unsigned)(hi - lo));
     bulk_g2s(smem + (size_t)(c % kStages) * T.stage, T.stream + lo, (unsigned)(hi - lo), b);
     lo = hi;
-    if (c + 2 <= T.nch) hi = T.off[c + 2];
+    if (c + 2 <= T.nch) hi = offs[c + 2];
   };
   if (tid == producer)
     for (int c = 0; c < kStages - 1 && c < T.nch; c++) issue(c);
@@ -472,7 +533,17 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
     const int s = c % kStages;
     if (c > 0 && !mbar_wait(&bar[s], (unsigned)((c / kStages) & 1))) abort_flag = 1;
     cp_async_wait_all();  // this thread's copies for chunk c have landed
-    __syncthreads();      // chunk c-1 solved; its stage and xbuf[(c+1)&1] are free
+    __syncthreads();      // this CTA's half of chunk c-1 solved; its stage and xbuf[(c+1)&1] are free
+    if (c > 0 && split) {
+      // meet the partner: its half of chunk c-1 (global x, ring rows in
+      // this CTA) is complete and visible once its arrival is seen
+      if (tid == 0) {
+        const unsigned slot = (unsigned)((c - 1) & 1);
+        mbar_arrive_remote(pxbar + 8u * slot);
+        if (!mbar_wait_cluster(&xbar[slot], (unsigned)(((c - 1) >> 1) & 1))) abort_flag = 1;
+      }
+      __syncthreads();
+    }
     if (abort_flag) break;
     const unsigned char* st = smem + (size_t)s * T.stage;
     const int4 h0 = reinterpret_cast<const int4*>(st)[0];
@@ -510,7 +581,7 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
     // near entries: results of chunk c-1 from the ring
     {
       const double2* rp =
-          reinterpret_cast<const double2*>(ring + 6 * (size_t)T.capr * ((c + 1) & 1));
+          reinterpret_cast<const double2*>(ring + 6 * (size_t)ringrows * ((c + 1) & 1));
       double2* xs2 = reinterpret_cast<double2*>(xs);
       for (int t = tid; t < 3 * nn; t += kSweepThreads) {
         const int2 q = nearl[t / 3];
@@ -527,10 +598,11 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
       }
       issued++;
     }
-    double* wp = ring + 6 * (size_t)T.capr * (c & 1);
+    double* wp = ring + 6 * (size_t)ringrows * (c & 1);
+    const unsigned pwp = pring + 8u * 6u * (unsigned)ringrows * (unsigned)(c & 1);
     for (int k = warp; k < nr && warp < nw - 1; k += nw - 1) {
       const int4 row = ri[k];
-      const int i = row.x, rbeg = row.y, rcnt = row.z;
+      const int i = row.x, rbeg = row.y, rcnt = row.z, gk = row.w;
       const int first = UPPER ? 1 : 0;  // U rows start with U_ii^{-1}
       double acc = 0.0;
       if (g < 4) {
@@ -558,17 +630,43 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
       }
       if (lane < 6) {
         ob[6 * (size_t)i + lane] = v;
-        wp[6 * k + lane] = v;
+        wp[6 * gk + lane] = v;
+        if (split) cluster_store(pwp + 8u * (unsigned)(6 * gk + lane), v);
       }
     }
   }
   cp_async_wait_all();  // no copy may land after the kernel ends
-  if (!abort_flag && tid == 0 && bytes_ctr) atomicAdd(bytes_ctr, (unsigned long long)T.abytes);
+  if (!abort_flag && tid == 0 && rank == 0 && bytes_ctr)
+    atomicAdd(bytes_ctr, (unsigned long long)T.abytes);
   if (abort_flag && tid == producer) {
     atomicOr(&ctl->status, ST_TIMEOUT);
     // chunks c .. issued-1 may still be in flight: let them land (bounded)
     for (int q = c; q < issued; q++) mbar_wait(&bar[q % kStages], (unsigned)((q / kStages) & 1));
   }
+  // neither CTA leaves while the other may still write into its shared
+  // memory; every path of both CTAs of a split problem reaches this point
+  if (split) cluster_barrier();
+}
+
+// One sweep of a batch: a cluster of kSweepCta CTAs per problem.
+template <class VT, bool UPPER>
+static cudaError_t launch_sweep(int np, size_t smem, cudaStream_t st, const ProbDev* desc,
+                                const int* live, const double* rhs, double* out, SweepCtl* ctl,
+                                unsigned long long* ctr) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(np * kSweepCta));
+  cfg.blockDim = dim3(kSweepThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = kSweepCta;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  ::gf::count_launch();
+  return cudaLaunchKernelEx(&cfg, bsweep_tma<VT, UPPER>, desc, live, rhs, out, ctl, ctr);
 }
 
 // Factor values into a chunk stream: block slot q of the triangle takes
@@ -833,7 +931,7 @@ struct gf_precond {
   DevBuf<int32_t> d_levLptr, d_levLrows;  // factorization order
   DevBuf<double> d_lu;
   struct Tri {
-    int nch = 0, stage = 0, capb = 0, capr = 0;
+    int nch = 0, stage = 0, capb = 0, capr = 0, nsplit = 1;
     size_t nslots = 0;
     long long abytes = 0;
     DevBuf<int64_t> off, vpos;
@@ -860,128 +958,174 @@ static cudaError_t build_tri(gf_precond* p, const std::vector<int32_t>& diag, bo
     for (int i = 0; i < n; i++) rows[f[lv[i]]++] = i;
   }
   int maxc = 0;
-  for (int i = 0; i < n; i++) maxc = std::max(maxc, cnt(i));
-  const int capb = std::max(p->prec == GF_PREC_FP32 ? 416 : 208, (maxc + 3) & ~3);
+  long long real = 0;
+  for (int i = 0; i < n; i++) {
+    maxc = std::max(maxc, cnt(i));
+    real += cnt(i);
+  }
+  const int mc4 = (maxc + 3) & ~3;
+  // Levels of more than ~200 blocks on average are split over the two CTAs
+  // of the problem's cluster: measured on B200, a chunk costs ~1.1 us plus
+  // ~4.7 ns a block on one CTA, and ~1.6 us plus ~2.3 ns a block when two
+  // CTAs share it and meet once per chunk.
+  const int nsplit = real > 200ll * std::max(nlev, 1) ? kSweepCta : 1;
+  const int base = p->prec == GF_PREC_FP32 ? 416 : 208;
   const int capr = 128;
-  // pass 1: chunk boundaries (row ranges of `rows`) and block counts
-  std::vector<int32_t> ck{0}, cb;  // chunk row starts, padded block counts
+  // per CTA: blocks of one half chunk. Split chunks are bounded so that
+  // giving each row to the lighter half leaves every half within capb (a
+  // half exceeds the mean by at most half a row) and a longest row fits.
+  const int capb = nsplit > 1 ? std::max(base, ((3 * mc4 + 1) / 2 + 3) & ~3) : std::max(base, mc4);
+  const int gcapb = nsplit > 1 ? nsplit * (capb - mc4) : capb, gcapr = nsplit * capr;
+  // pass 1: chunk boundaries (row ranges of `rows`); a chunk never spans two levels
+  std::vector<int32_t> ck{0};
   {
     int cur = 0, nr = 0;
-    auto close = [&](int k) {
-      cur = std::max(4, (cur + 3) & ~3);
-      ck.push_back(k);
-      cb.push_back(cur);
-      cur = nr = 0;
-    };
     for (int l = 0; l < nlev; l++) {
       for (int k = ptr[l]; k < ptr[l + 1]; k++) {
         const int c = cnt(rows[k]);
-        if (nr > 0 && (cur + c > capb || nr == capr)) close(k);
+        if (nr > 0 && (cur + c > gcapb || nr == gcapr)) {
+          ck.push_back(k);
+          cur = nr = 0;
+        }
         cur += c;
         nr++;
       }
-      if (nr > 0) close(ptr[l + 1]);  // a chunk never spans two levels
+      if (nr > 0) {
+        ck.push_back(ptr[l + 1]);
+        cur = nr = 0;
+      }
     }
   }
-  const int nch = (int)cb.size();
-  // chunk and chunk-local index of every row
-  std::vector<int32_t> chunk_of(n), local(n);
-  for (int c = 0; c < nch; c++)
-    for (int k = ck[c]; k < ck[c + 1]; k++) {
-      chunk_of[rows[k]] = c;
-      local[rows[k]] = k - ck[c];
-    }
-  // per chunk: where each stored block's x comes from. Near: row solved by
-  // the previous chunk (ring, chunk-local row); far: solved earlier (global
-  // row). U's diagonal block U_ii^{-1} multiplies no x; padding is unused.
-  std::vector<std::vector<int32_t>> nearl(nch), farl(nch);  // pairs (slot, source)
+  const int nch = (int)ck.size() - 1;
+  // split every chunk's rows over the CTAs: each row goes to the half with
+  // fewer blocks so far (ties: fewer rows), within capr rows a half
+  std::vector<int32_t> half(n), chunk_of(n), grow(n);
+  std::vector<std::vector<int32_t>> hrows((size_t)kSweepCta * nch);  // [h * nch + c]
   for (int c = 0; c < nch; c++) {
-    int b = 0;
-    auto src = [&](int slot, int j) {
-      const int pc = chunk_of[j];
-      if (pc == c - 1) {
-        nearl[c].push_back(slot);
-        nearl[c].push_back(local[j]);
-      } else {
-        farl[c].push_back(slot);
-        farl[c].push_back(j);
-      }
-    };
+    int hb[kSweepCta] = {0}, hr[kSweepCta] = {0};
     for (int k = ck[c]; k < ck[c + 1]; k++) {
       const int i = rows[k];
-      if (upper) {
-        b++;  // U_ii^{-1}
-        for (int jp = diag[i] + 1; jp < P.rowp[i + 1]; jp++) src(b++, P.cols[jp]);
-      } else {
-        for (int jp = P.rowp[i]; jp < diag[i]; jp++) src(b++, P.cols[jp]);
-      }
+      int h = 0;
+      for (int q = 1; q < nsplit; q++)
+        if (hr[h] == capr || (hr[q] < capr && (hb[q] < hb[h] || (hb[q] == hb[h] && hr[q] < hr[h]))))
+          h = q;
+      half[i] = h;
+      chunk_of[i] = c;
+      grow[i] = k - ck[c];
+      hb[h] += cnt(i);
+      hr[h]++;
+      hrows[(size_t)h * nch + c].push_back(i);
     }
+    for (int h = 0; h < kSweepCta; h++)
+      if (hb[h] > capb || hr[h] > capr) return cudaErrorInvalidValue;
   }
-  if (!farl[0].empty() || !nearl[0].empty()) return cudaErrorInvalidValue;  // level 0 has none
-  // byte layout of chunk c: two int4 headers, row records, near list, the
-  // far list and row indices of chunk c+1, then (16-byte aligned) values
-  auto pre = [&](int c) {
-    const int64_t nr = ck[c + 1] - ck[c];
-    const int64_t nf1 = c + 1 < nch ? (int64_t)farl[c + 1].size() / 2 : 0;
-    const int64_t nr1 = c + 1 < nch ? ck[c + 2] - ck[c + 1] : 0;
-    return (32 + 16 * nr + 4 * (int64_t)nearl[c].size() + 8 * nf1 + 4 * nr1 + 15) & ~(int64_t)15;
+  // per half chunk: stored blocks (padded), and where each block's x comes
+  // from. Near: row solved by the previous chunk (either CTA; ring position
+  // = its row index within that chunk); far: solved earlier (global row).
+  // U's diagonal block U_ii^{-1} multiplies no x; padding is unused.
+  const size_t HC = (size_t)kSweepCta * nch;
+  std::vector<int32_t> nbp(HC);
+  std::vector<std::vector<int32_t>> nearl(HC), farl(HC);  // pairs (slot, source)
+  for (int h = 0; h < kSweepCta; h++)
+    for (int c = 0; c < nch; c++) {
+      const size_t hc = (size_t)h * nch + c;
+      int b = 0;
+      auto src = [&](int slot, int j) {
+        if (chunk_of[j] == c - 1) {
+          nearl[hc].push_back(slot);
+          nearl[hc].push_back(grow[j]);
+        } else {
+          farl[hc].push_back(slot);
+          farl[hc].push_back(j);
+        }
+      };
+      for (int i : hrows[hc]) {
+        if (upper) {
+          b++;  // U_ii^{-1}
+          for (int jp = diag[i] + 1; jp < P.rowp[i + 1]; jp++) src(b++, P.cols[jp]);
+        } else {
+          for (int jp = P.rowp[i]; jp < diag[i]; jp++) src(b++, P.cols[jp]);
+        }
+      }
+      nbp[hc] = std::max(4, (b + 3) & ~3);
+    }
+  for (int h = 0; h < kSweepCta; h++)
+    if (!farl[(size_t)h * nch].empty() || !nearl[(size_t)h * nch].empty())
+      return cudaErrorInvalidValue;  // level 0 depends on nothing
+  // byte layout of half chunk (h, c): two int4 headers, row records {row,
+  // first block, blocks, row index in the chunk}, the near list, the far
+  // list and rows of half chunk (h, c+1), then (16-byte aligned) values.
+  // Half h's chunks are contiguous; off[h * (nch + 1) + c] is their start.
+  auto pre = [&](int h, int c) {
+    const size_t hc = (size_t)h * nch + c;
+    const int64_t nr = (int64_t)hrows[hc].size();
+    const int64_t nf1 = c + 1 < nch ? (int64_t)farl[hc + 1].size() / 2 : 0;
+    const int64_t nr1 = c + 1 < nch ? (int64_t)hrows[hc + 1].size() : 0;
+    return (32 + 16 * nr + 4 * (int64_t)nearl[hc].size() + 8 * nf1 + 4 * nr1 + 15) & ~(int64_t)15;
   };
-  std::vector<int64_t> off(nch + 1, 0);
+  std::vector<int64_t> off((size_t)kSweepCta * (nch + 1), 0);
   size_t nslots = 0;
   int stage = 0;
-  for (int c = 0; c < nch; c++) {
-    const int64_t bytes = pre(c) + 36 * (int64_t)vs * cb[c];
-    off[c + 1] = off[c] + bytes;
-    stage = std::max<int64_t>(stage, bytes);
-    nslots += cb[c];
-  }
-  std::vector<unsigned char> bytes(off[nch], 0);
+  int64_t pos = 0;
+  for (int h = 0; h < kSweepCta; h++)
+    for (int c = 0; c <= nch; c++) {
+      off[(size_t)h * (nch + 1) + c] = pos;
+      if (c == nch) break;
+      const int64_t bytes = pre(h, c) + 36 * (int64_t)vs * nbp[(size_t)h * nch + c];
+      pos += bytes;
+      stage = (int)std::max<int64_t>(stage, bytes);
+      nslots += nbp[(size_t)h * nch + c];
+    }
+  std::vector<unsigned char> bytes(pos, 0);
   std::vector<int32_t> map(nslots, -1);
   std::vector<int64_t> vpos(nslots);
   size_t q = 0;
-  for (int c = 0; c < nch; c++) {
-    int32_t* w = reinterpret_cast<int32_t*>(bytes.data() + off[c]);
-    const int nr = ck[c + 1] - ck[c], nb = cb[c];
-    const int nn = (int)nearl[c].size() / 2;
-    const int nf1 = c + 1 < nch ? (int)farl[c + 1].size() / 2 : 0;
-    const int nr1 = c + 1 < nch ? ck[c + 2] - ck[c + 1] : 0;
-    w[0] = nr;
-    w[1] = nb;
-    w[2] = nn;
-    w[4] = nf1;
-    w[5] = nr1;
-    int32_t* rec = w + 8;
-    int b = 0;
-    for (int k = ck[c]; k < ck[c + 1]; k++) {
-      const int i = rows[k];
-      rec[4 * (k - ck[c]) + 0] = i;
-      rec[4 * (k - ck[c]) + 1] = b;
-      rec[4 * (k - ck[c]) + 2] = cnt(i);
-      if (upper) {
-        map[q + b++] = diag[i];
-        for (int jp = diag[i] + 1; jp < P.rowp[i + 1]; jp++) map[q + b++] = jp;
-      } else {
-        for (int jp = P.rowp[i]; jp < diag[i]; jp++) map[q + b++] = jp;
+  for (int h = 0; h < kSweepCta; h++)
+    for (int c = 0; c < nch; c++) {
+      const size_t hc = (size_t)h * nch + c;
+      const int64_t o = off[(size_t)h * (nch + 1) + c];
+      int32_t* w = reinterpret_cast<int32_t*>(bytes.data() + o);
+      const int nr = (int)hrows[hc].size(), nb = nbp[hc];
+      const int nn = (int)nearl[hc].size() / 2;
+      const int nf1 = c + 1 < nch ? (int)farl[hc + 1].size() / 2 : 0;
+      const int nr1 = c + 1 < nch ? (int)hrows[hc + 1].size() : 0;
+      w[0] = nr;
+      w[1] = nb;
+      w[2] = nn;
+      w[4] = nf1;
+      w[5] = nr1;
+      int32_t* rec = w + 8;
+      int b = 0;
+      for (int k = 0; k < nr; k++) {
+        const int i = hrows[hc][k];
+        rec[4 * k + 0] = i;
+        rec[4 * k + 1] = b;
+        rec[4 * k + 2] = cnt(i);
+        rec[4 * k + 3] = grow[i];
+        if (upper) {
+          map[q + b++] = diag[i];
+          for (int jp = diag[i] + 1; jp < P.rowp[i + 1]; jp++) map[q + b++] = jp;
+        } else {
+          for (int jp = P.rowp[i]; jp < diag[i]; jp++) map[q + b++] = jp;
+        }
       }
+      int32_t* lists = rec + 4 * nr;
+      std::copy(nearl[hc].begin(), nearl[hc].end(), lists);
+      lists += nearl[hc].size();
+      if (c + 1 < nch) {
+        std::copy(farl[hc + 1].begin(), farl[hc + 1].end(), lists);
+        lists += farl[hc + 1].size();
+        for (int i : hrows[hc + 1]) *lists++ = i;
+      }
+      const int64_t v0 = (o + pre(h, c)) / (int64_t)vs;
+      for (int k = 0; k < nb; k++) vpos[q + k] = v0 + 36 * (int64_t)k;
+      q += nb;
     }
-    int32_t* lists = rec + 4 * nr;
-    std::copy(nearl[c].begin(), nearl[c].end(), lists);
-    lists += nearl[c].size();
-    if (c + 1 < nch) {
-      std::copy(farl[c + 1].begin(), farl[c + 1].end(), lists);
-      lists += farl[c + 1].size();
-      for (int k = ck[c + 1]; k < ck[c + 2]; k++) *lists++ = rows[k];
-    }
-    const int64_t v0 = (off[c] + pre(c)) / (int64_t)vs;
-    for (int k = 0; k < nb; k++) vpos[q + k] = v0 + 36 * (int64_t)k;
-    q += nb;
-  }
   // algorithmic bytes of one sweep: per stored block its values, column
   // index and the 6 x entries it multiplies; per row a row pointer, its
   // right-hand side and its result
-  long long real = 0;
-  for (int i = 0; i < n; i++) real += cnt(i);
   gf_precond::Tri& t = p->tri[upper ? 1 : 0];
+  t.nsplit = nsplit;
   t.abytes = real * (36 * (long long)vs + 4 + 48) + (long long)n * (4 + 48 + 48);
   t.nch = nch;
   t.stage = stage;
@@ -1000,7 +1144,7 @@ static cudaError_t build_tri(gf_precond* p, const std::vector<int32_t>& diag, bo
 }
 static TriDesc tri_desc(const gf_precond* p, int which) {
   const gf_precond::Tri& t = p->tri[which];
-  return TriDesc{t.nch, t.stage, t.capb, t.capr, t.off.p, t.stream.p, t.abytes};
+  return TriDesc{t.nch, t.stage, t.capb, t.capr, t.off.p, t.stream.p, t.abytes, t.nsplit};
 }
 static size_t sweep_smem(const gf_precond* p, int which) {
   const gf_precond::Tri& t = p->tri[which];
@@ -1239,10 +1383,10 @@ static gf_status bsweeps(gf_batch* B, const int* live, const double* r, double* 
   unsigned long long* ctr = nullptr;
   cudaEvent_t e1 = nullptr;
   if (timing_begin(st, &ctr, &e1) != GF_OK) return GF_CUDA_ERROR;
-  bsweep_tma<VT, false><<<B->np, kSweepThreads, B->smemL, st>>>(B->d_desc.p, live, r, B->d_tmp.p,
-                                                                B->d_ctl.p, ctr); ::gf::count_launch();
-  bsweep_tma<VT, true><<<B->np, kSweepThreads, B->smemU, st>>>(B->d_desc.p, live, B->d_tmp.p, z,
-                                                               B->d_ctl.p, ctr); ::gf::count_launch();
+  GF_CUDA((launch_sweep<VT, false>(B->np, B->smemL, st, B->d_desc.p, live, r, B->d_tmp.p,
+                                    B->d_ctl.p, ctr)));
+  GF_CUDA((launch_sweep<VT, true>(B->np, B->smemU, st, B->d_desc.p, live, B->d_tmp.p, z,
+                                   B->d_ctl.p, ctr)));
   GF_CHECK_LAUNCH();
   if (e1) GF_CUDA(cudaEventRecord(e1, st));
   return GF_OK;
@@ -1745,23 +1889,19 @@ gf_status gf_precond_apply_noalloc(gf_precond* p, const double* d_r, double* d_z
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSweepSmemMax));
     GF_CUDA(cudaFuncSetAttribute(bsweep_tma<float, true>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSweepSmemMax));
-    bsweep_tma<float, false><<<1, kSweepThreads, B->smemL, st>>>(B->d_desc.p, nullptr, d_r, y,
-                                                                 B->d_ctl.p, nullptr);
-    ::gf::count_launch();
-    bsweep_tma<float, true><<<1, kSweepThreads, B->smemU, st>>>(B->d_desc.p, nullptr, y, d_z,
-                                                                B->d_ctl.p, nullptr);
-    ::gf::count_launch();
+    GF_CUDA((launch_sweep<float, false>(1, B->smemL, st, B->d_desc.p, nullptr, d_r, y,
+                                        B->d_ctl.p, nullptr)));
+    GF_CUDA((launch_sweep<float, true>(1, B->smemU, st, B->d_desc.p, nullptr, y, d_z, B->d_ctl.p,
+                                       nullptr)));
   } else {
     GF_CUDA(cudaFuncSetAttribute(bsweep_tma<double, false>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSweepSmemMax));
     GF_CUDA(cudaFuncSetAttribute(bsweep_tma<double, true>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSweepSmemMax));
-    bsweep_tma<double, false><<<1, kSweepThreads, B->smemL, st>>>(B->d_desc.p, nullptr, d_r, y,
-                                                                  B->d_ctl.p, nullptr);
-    ::gf::count_launch();
-    bsweep_tma<double, true><<<1, kSweepThreads, B->smemU, st>>>(B->d_desc.p, nullptr, y, d_z,
-                                                                 B->d_ctl.p, nullptr);
-    ::gf::count_launch();
+    GF_CUDA((launch_sweep<double, false>(1, B->smemL, st, B->d_desc.p, nullptr, d_r, y,
+                                         B->d_ctl.p, nullptr)));
+    GF_CUDA((launch_sweep<double, true>(1, B->smemU, st, B->d_desc.p, nullptr, y, d_z, B->d_ctl.p,
+                                        nullptr)));
   }
   GF_CHECK_LAUNCH();
   return GF_OK;
