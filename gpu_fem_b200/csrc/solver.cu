@@ -43,6 +43,98 @@ struct SweepCtl {
   int pivot;
 };
 
+// ------------------------------------------------ barriers and bulk copies
+constexpr unsigned long long kWaitNs = 2000000000ull;  // bound of every device-side wait
+constexpr int kSweepCta = 2;  // CTAs (one thread-block cluster) per problem for triangular work
+
+__device__ __forceinline__ unsigned long long gtimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait; returns false if kWaitNs passed first
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+  const unsigned long long t0 = gtimer();
+  unsigned n = 0;
+  while (!mbar_try_wait(bar, parity)) {
+    if ((++n & 255u) == 0u && gtimer() - t0 > kWaitNs) return false;
+  }
+  return true;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes,
+                                         uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ unsigned cluster_rank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+// address of the same shared-memory location in CTA `rank` of the cluster
+__device__ __forceinline__ unsigned cluster_map(unsigned addr, unsigned rank) {
+  unsigned r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void cluster_store(unsigned addr, double v) {
+  asm volatile("st.shared::cluster.f64 [%0], %1;" ::"r"(addr), "d"(v) : "memory");
+}
+// arrive on an mbarrier of another CTA of the cluster (releases this CTA's
+// earlier writes at cluster scope)
+__device__ __forceinline__ void mbar_arrive_remote(unsigned addr) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(addr)
+               : "memory");
+}
+// bounded wait with acquire at cluster scope; false if kWaitNs passed first
+__device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, unsigned parity) {
+  const unsigned long long t0 = gtimer();
+  unsigned n = 0;
+  while (true) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if ((++n & 255u) == 0u && gtimer() - t0 > kWaitNs) return false;
+  }
+}
+// all threads of all CTAs of the cluster
+__device__ __forceinline__ void cluster_barrier() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\nbarrier.cluster.wait.acquire.aligned;" :::
+                   "memory");
+}
+
+
 // ------------------------------------------------------------------ SpMV
 // y = alpha A x + beta y over all rows of live problems; one warp per block
 // row, 4 groups of 6 lanes (group g takes blocks g, g+4, ...).
@@ -155,22 +247,44 @@ __device__ __forceinline__ int find_col(const int32_t* c, int lo, int hi, int j)
   return (lo < end && c[lo] == j) ? lo : -1;
 }
 
+// Problems with many rows per level factor each level on both CTAs of a
+// thread-block cluster (rows alternate between their warps); the CTAs meet
+// after every level on a pair of mbarriers (remote arrive with release,
+// bounded wait with acquire, at cluster scope) and end on a cluster barrier
+// that every path reaches. Other problems run on the first CTA alone.
 __global__ void __launch_bounds__(kFacWarps * 32) bfactor_kernel(const ProbDev* __restrict__ P,
                                                                 SweepCtl* ctl) {
   __shared__ double sL[kFacWarps][36];
   __shared__ double sM[kFacWarps][36];
   __shared__ double sI[kFacWarps][36];
   __shared__ int32_t sC[kFacWarps][kFacRow];
+  __shared__ uint64_t fbar[2];  // the partner's "level done" arrivals, alternating
+  __shared__ int fabort;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   const int b = lane / 6, c = lane % 6;  // update slot and column (lanes 30, 31 idle)
-  const ProbDev d = P[blockIdx.x];
+  const unsigned rank = cluster_rank();
+  const ProbDev d = P[blockIdx.x / kSweepCta];
+  const bool split = d.fac_split != 0;
+  if (!split && rank != 0) return;
+  if (threadIdx.x == 0) {
+    mbar_init(&fbar[0], 1);
+    mbar_init(&fbar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    fabort = 0;
+  }
+  if (split)
+    cluster_barrier();
+  else
+    __syncthreads();
+  const unsigned pfbar = split ? cluster_map(smem_u32(fbar), rank ^ 1u) : 0u;
+  const int wbase = split ? (int)rank * nw + warp : warp, wstride = split ? 2 * nw : nw;
   const int32_t* rowp = d.prowp;
   const int32_t* cols = d.pcols;
   const int32_t* diag = d.pdiag;
   double* LU = d.LU64;
   double* Lb = sL[warp];
   for (int lev = 0; lev < d.nlevL; lev++) {
-    for (int idx = d.levLptr[lev] + warp; idx < d.levLptr[lev + 1]; idx += nw) {
+    for (int idx = d.levLptr[lev] + wbase; idx < d.levLptr[lev + 1]; idx += wstride) {
       const int i = d.levLrows[idx];
       const int r0 = rowp[i], r1 = rowp[i + 1], di = diag[i], len = r1 - r0;
       const bool staged = len <= kFacRow;
@@ -264,7 +378,22 @@ __global__ void __launch_bounds__(kFacWarps * 32) bfactor_kernel(const ProbDev* 
       __syncwarp();
     }
     __syncthreads();
+    if (split) {
+      // both CTAs' rows of this level are final before either starts the next
+      if (threadIdx.x == 0) {
+        const unsigned slot = (unsigned)(lev & 1);
+        mbar_arrive_remote(pfbar + 8u * slot);
+        if (!mbar_wait_cluster(&fbar[slot], (unsigned)((lev >> 1) & 1))) {
+          fabort = 1;
+          atomicOr(&ctl->status, ST_TIMEOUT);
+        }
+      }
+      __syncthreads();
+      if (fabort) break;
+    }
   }
+  // no CTA leaves while its partner may still arrive on its barriers
+  if (split) cluster_barrier();
 }
 
 __global__ void scatter_values_kernel(int nA, const int32_t* __restrict__ map,
@@ -299,97 +428,8 @@ __global__ void convert_kernel(size_t n, const double* __restrict__ in, T2* __re
 // its rows' 6x6 products. x / y live in global memory, written and re-read
 // by the problem's cluster only.
 constexpr int kSweepThreads = 512;
-constexpr int kSweepCta = 2;  // CTAs (one thread-block cluster) per problem and sweep
 constexpr int kStages = 2;
-constexpr unsigned long long kWaitNs = 2000000000ull;
 constexpr size_t kSweepSmemMax = 220 * 1024;  // dynamic; the static part is < 1 KB
-
-__device__ __forceinline__ unsigned long long gtimer() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-__device__ __forceinline__ unsigned smem_u32(const void* p) {
-  return (unsigned)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
-               : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-               "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
-  unsigned ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      " selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// bounded wait; returns false if kWaitNs passed first
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
-  const unsigned long long t0 = gtimer();
-  unsigned n = 0;
-  while (!mbar_try_wait(bar, parity)) {
-    if ((++n & 255u) == 0u && gtimer() - t0 > kWaitNs) return false;
-  }
-  return true;
-}
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes,
-                                         uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
-          "r"(smem_u32(dst)),
-      "l"(src), "r"(bytes), "r"(smem_u32(bar))
-      : "memory");
-}
-
-__device__ __forceinline__ unsigned cluster_rank() {
-  unsigned r;
-  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-  return r;
-}
-// address of the same shared-memory location in CTA `rank` of the cluster
-__device__ __forceinline__ unsigned cluster_map(unsigned addr, unsigned rank) {
-  unsigned r;
-  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
-  return r;
-}
-__device__ __forceinline__ void cluster_store(unsigned addr, double v) {
-  asm volatile("st.shared::cluster.f64 [%0], %1;" ::"r"(addr), "d"(v) : "memory");
-}
-// arrive on an mbarrier of another CTA of the cluster (releases this CTA's
-// earlier writes at cluster scope)
-__device__ __forceinline__ void mbar_arrive_remote(unsigned addr) {
-  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(addr)
-               : "memory");
-}
-// bounded wait with acquire at cluster scope; false if kWaitNs passed first
-__device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, unsigned parity) {
-  const unsigned long long t0 = gtimer();
-  unsigned n = 0;
-  while (true) {
-    unsigned ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    if (ok) return true;
-    if ((++n & 255u) == 0u && gtimer() - t0 > kWaitNs) return false;
-  }
-}
-// all threads of all CTAs of the cluster
-__device__ __forceinline__ void cluster_barrier() {
-  asm volatile("barrier.cluster.arrive.release.aligned;\nbarrier.cluster.wait.acquire.aligned;" :::
-                   "memory");
-}
 
 // Dynamic shared memory of one sweep: kStages staging buffers of `stage`
 // bytes; two buffers (this chunk, next chunk) of gathered x (capb x 6
@@ -1204,6 +1244,8 @@ static gf_status upload_desc(gf_batch* B) {
     d.pdiag = p->d_diag.p;
     d.LU64 = p->d_lu.p;
     d.nlevL = p->nlevL;
+    // two CTAs per level pay off once a level has more rows than one CTA's warps
+    d.fac_split = p->pat.n > 16 * std::max(p->nlevL, 1) ? 1 : 0;
     d.nlevU = p->nlevU;
     d.levLptr = p->d_levLptr.p;
     d.levLrows = p->d_levLrows.p;
@@ -1425,7 +1467,23 @@ static gf_status batch_factor(gf_batch* B, cudaStream_t st) {
   }
   GF_CHECK_LAUNCH();
   GF_CUDA(cudaMemsetAsync(&B->d_ctl.p->status, 0, 2 * sizeof(int), st));
-  bfactor_kernel<<<B->np, kFacWarps * 32, 0, st>>>(B->d_desc.p, B->d_ctl.p); ::gf::count_launch();
+  {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(B->np * kSweepCta));
+    cfg.blockDim = dim3(kFacWarps * 32);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kSweepCta;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const ProbDev* desc = B->d_desc.p;
+    SweepCtl* ctl = B->d_ctl.p;
+    ::gf::count_launch();
+    GF_CUDA(cudaLaunchKernelEx(&cfg, bfactor_kernel, desc, ctl));
+  }
   GF_CHECK_LAUNCH();
   for (int k = 0; k < B->np; k++) {
     gf_precond* p = B->pcs[k];
