@@ -83,16 +83,21 @@ ORDERINGS = ("natural", "rcm")
 def step_cost_us(nrow, inf, iterations):
     """Critical-path model of one factor + solve of a problem (microseconds),
     fitted to B200 runs of the 64-plate batch. The factorization walks its
-    lower levels in rounds of 16 rows (one per warp); a row's steps are
+    lower levels in rounds of one row per warp (16 warps, or 32 when levels
+    average more than 16 rows and two CTAs share them); a row's steps are
     sequential and each updates about one row length of blocks, so a row
     costs ~0.35 us x (lower blocks)^2. Every GMRES step runs both sweeps at
-    ~1.1 us a level plus ~9 ns per block of the level, and ~30 us of SpMV and
-    reductions."""
+    ~1.1 us a level plus ~9 ns per block of the level, or ~1.6 us plus
+    ~4.5 ns when levels average more than 200 blocks and two CTAs share
+    them, and ~30 us of SpMV and reductions."""
     lvl, lvu, nnzb = inf["levels_L"], inf["levels_U"], inf["nnzb"]
     lower = max(nnzb - nrow, 0) / (2.0 * nrow)
-    rounds = -(-nrow // max(lvl, 1) // 16) or 1
+    rows_per_level = nrow / max(lvl, 1)
+    warps = 32 if rows_per_level > 16 else 16
+    rounds = max(1, -(-int(rows_per_level) // warps))
     factor = lvl * rounds * 0.35 * lower * lower
-    per_level = 1.1 + 0.009 * max(nnzb - nrow, 0) / 2.0 / max(lvl, 1)
+    blocks = max(nnzb - nrow, 0) / 2.0 / max(lvl, 1)
+    per_level = 1.6 + 0.0045 * blocks if blocks > 200 else 1.1 + 0.009 * blocks
     return factor + iterations * ((lvl + lvu) * per_level + 30.0)
 
 
