@@ -51,7 +51,7 @@ def _args():
                          "jittered cantilever plate, 5 times (no JSON line)")
     ap.add_argument("--sweep-case", action="store_true",
                     help="small profiling case: the triangular sweeps of one 256x128 plate, "
-                         "ILU(6), FP32 factors, applied 5 times (no JSON line)")
+                         "natural ordering, ILU(6), FP32 factors, applied 5 times (no JSON line)")
     return ap.parse_args()
 
 
@@ -100,15 +100,16 @@ def assembly_case():
 
 
 def sweep_case():
-    """One preconditioner (256x128 clamped plate, t = 2 mm, RCM, ILU(6), FP32
-    factors, ~150 MB of factor) applied 5 times: the small case on which the
-    sweep kernel is profiled."""
+    """One preconditioner (256x128 clamped plate, t = 2 mm, natural ordering,
+    ILU(6), FP32 factors, ~150 MB of factor) applied 5 times: the small case
+    on which the sweep and factorization kernels are profiled (its levels
+    are large enough that both run on a two-CTA cluster)."""
     import torch
     from gpu_fem_b200 import mesh as M
     from gpu_fem_b200.assembler import ElementAssembler, ILUk_Preconditioner, createBsrMat
     m = M.plate(256, 128, 1.0, 0.5, lambda x, y: 0.002 + 0 * x, "all_edges",
                 lambda q: 1e3 + 0 * q[:, 0])
-    A = ElementAssembler.from_mesh(m, ordering="rcm")
+    A = ElementAssembler.from_mesh(m, ordering="natural")
     K = createBsrMat(A)
     A.add_jacobian(None, K, fuse_bcs=True)
     P = ILUk_Preconditioner(A, fill_level=6, precision="fp32")
