@@ -173,3 +173,29 @@ def test_precond_apply_accepts_8_byte_aligned_vectors():
         P.apply(rb[1:], zb[1:])  # both vectors 8 bytes off a 16-byte boundary
         torch.cuda.synchronize()
         assert np.array_equal(z.cpu().numpy().view(np.uint64), zb[1:].cpu().numpy().view(np.uint64))
+
+
+def test_status_codes_zero_pivot_and_not_converged():
+    """A singular diagonal block is reported as GF_ZERO_PIVOT (no fault), and
+    an iteration cap that is too small as GF_NOT_CONVERGED with the achieved
+    residual."""
+    import torch
+    from gpu_fem_b200 import _lib as L
+    from gpu_fem_b200.assembler import (ElementAssembler, ILUk_Preconditioner, SolveOptions,
+                                        createBsrMat, gmres_solve)
+    mesh = M.plate_config2(24, 12)
+    A = ElementAssembler.from_mesh(mesh, ordering="rcm")
+    K = createBsrMat(A)
+    K.zeroValues()  # every block zero: the first pivot block is singular
+    P = ILUk_Preconditioner(A, fill_level=0)
+    with pytest.raises(L.GpuFemError) as err:
+        P.factor(K)
+    assert err.value.status == L.GF_ZERO_PIVOT
+    A.add_jacobian(None, K, fuse_bcs=True)
+    P.factor(K)  # the context is still usable
+    b = torch.tensor(mesh.loads, device="cuda")
+    x = torch.zeros_like(b)
+    st, stats = gmres_solve(A, K, P, b, x, SolveOptions(restart=10, max_iters=3, rtol=1e-12,
+                                                        side=1), raise_on_fail=False)
+    assert st == L.GF_NOT_CONVERGED
+    assert stats["iterations"] <= 3 and stats["rel_residual"] > 1e-12
