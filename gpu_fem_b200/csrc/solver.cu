@@ -1852,6 +1852,9 @@ gf_status gf_precond_create(gf_assembler* a, int32_t fill_level, int32_t precisi
     return sweep_smem(p, w) <= kSweepSmemMax;
   };
   if (e == cudaSuccess && !(fits(0) && fits(1))) {
+    set_last_error_text("gf_precond_create: the ILU(" + std::to_string(fill_level) +
+                        ") factor has rows too long for the triangular sweep's "
+                        "shared-memory stage; use a lower fill level");
     delete p;
     return GF_INVALID_ARG;  // a factor row longer than one staging buffer
   }

@@ -171,8 +171,10 @@ enum { GF_PREC_FP64 = 0, GF_PREC_FP32 = 1 };
 /* ILUk_Preconditioner (include/linalg/precond.h:5-55) with the symbolic
  * ILU(k) of computeILUk (include/linalg/bsr_utils.h:678-807); fill_level 0
  * keeps A's pattern (ILU(0)). precision selects FP64 or FP32 factors.
- * GF_INVALID_ARG if a factor row holds more blocks than one shared-memory
- * stage of the triangular sweep (about 240 blocks in FP64, 400 in FP32). */
+ * Fails (GF_INVALID_ARG or GF_CUDA_ERROR with the reason in gf_last_error)
+ * if a factor row holds more blocks than one shared-memory stage of the
+ * triangular sweep: about 260 blocks in FP64 and 440 in FP32, or 170 and
+ * 290 for triangles whose levels are split over two CTAs. */
 gf_status gf_precond_create(gf_assembler* a, int32_t fill_level, int32_t precision,
                             gf_precond** out);
 gf_status gf_precond_destroy(gf_precond* p);
