@@ -744,19 +744,56 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
   return s;
 }
 
-// partial[i * C.n + c] = V_i . w over chunk c, i = 0..jj, for running problems
-__global__ void seg_dots(const double* __restrict__ V, const double* __restrict__ w, size_t N,
-                         int jj, Chunks C, const int* __restrict__ run, double* partial) {
-  __shared__ double sh[32];
+// partial[i * C.n + c] = V_i . w over chunk c, i = 0..jj, for running problems.
+// w stays in registers; eight basis vectors at a time are read with all
+// their loads in flight and reduced together (the same summation order as
+// one vector at a time: per thread in element order, then the warp tree,
+// then the warps in order).
+constexpr int kDotGroup = 8;
+__global__ void __launch_bounds__(kRedThreads) seg_dots(const double* __restrict__ V,
+                                                        const double* __restrict__ w, size_t N,
+                                                        int jj, Chunks C,
+                                                        const int* __restrict__ run,
+                                                        double* partial) {
+  constexpr int E = kChunk / kRedThreads;  // elements per thread
+  __shared__ double sh[kDotGroup][kRedThreads / 32];
   const int c = blockIdx.x;
   if (!run[C.prob[c]]) return;
   const int64_t lo = C.lo[c], hi = C.hi[c];
-  for (int i = 0; i <= jj; i++) {
-    const double* v = V + (size_t)i * N;
-    double acc = 0.0;
-    for (int64_t t = lo + threadIdx.x; t < hi; t += blockDim.x) acc = fma(v[t], w[t], acc);
-    const double s = block_sum(acc, sh);
-    if (threadIdx.x == 0) partial[(size_t)i * C.n + c] = s;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double wr[E];
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    const int64_t t = lo + threadIdx.x + (int64_t)e * kRedThreads;
+    wr[e] = t < hi ? w[t] : 0.0;
+  }
+  for (int i0 = 0; i0 <= jj; i0 += kDotGroup) {
+    double acc[kDotGroup];
+#pragma unroll
+    for (int q = 0; q < kDotGroup; q++) {
+      acc[q] = 0.0;
+      if (i0 + q <= jj) {
+        const double* v = V + (size_t)(i0 + q) * N;
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+          const int64_t t = lo + threadIdx.x + (int64_t)e * kRedThreads;
+          if (t < hi) acc[q] = fma(v[t], wr[e], acc[q]);
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kDotGroup; q++)
+      for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_down_sync(0xffffffffu, acc[q], o);
+    if (lane == 0)
+#pragma unroll
+      for (int q = 0; q < kDotGroup; q++) sh[q][warp] = acc[q];
+    __syncthreads();
+    if (threadIdx.x < kDotGroup && i0 + (int)threadIdx.x <= jj) {
+      double s = 0.0;
+      for (int k = 0; k < kRedThreads / 32; k++) s += sh[threadIdx.x][k];
+      partial[(size_t)(i0 + threadIdx.x) * C.n + c] = s;
+    }
+    __syncthreads();
   }
 }
 
@@ -801,6 +838,7 @@ __global__ void seg_update(const double* __restrict__ V, double* __restrict__ w,
   double acc = 0.0;
   for (int64_t t = lo + threadIdx.x; t < hi; t += blockDim.x) {
     double s = w[t];
+#pragma unroll 8
     for (int i = 0; i <= jj; i++) s = fma(-hs[i], V[(size_t)i * N + t], s);
     w[t] = s;
     acc = fma(s, s, acc);
