@@ -89,7 +89,8 @@ def step_cost_us(nrow, inf, iterations):
     costs ~0.35 us x (lower blocks)^2. Every GMRES step runs both sweeps at
     ~1.1 us a level plus ~9 ns per block of the level, or ~1.6 us plus
     ~4.5 ns when levels average more than 200 blocks and two CTAs share
-    them, and ~30 us of SpMV and reductions."""
+    them, and ~150 us of SpMV, reductions and launches (in a batch every
+    step of the slowest-converging problem keeps all of them running)."""
     lvl, lvu, nnzb = inf["levels_L"], inf["levels_U"], inf["nnzb"]
     lower = max(nnzb - nrow, 0) / (2.0 * nrow)
     rows_per_level = nrow / max(lvl, 1)
@@ -98,7 +99,7 @@ def step_cost_us(nrow, inf, iterations):
     factor = lvl * rounds * 0.35 * lower * lower
     blocks = max(nnzb - nrow, 0) / 2.0 / max(lvl, 1)
     per_level = 1.6 + 0.0045 * blocks if blocks > 200 else 1.1 + 0.009 * blocks
-    return factor + iterations * ((lvl + lvu) * per_level + 30.0)
+    return factor + iterations * ((lvl + lvu) * per_level + 150.0)
 
 
 def choose_ordering(mesh, fill=8):
