@@ -44,3 +44,22 @@ def test_batch_config4_seeded():
     sizes = [p.num_elements for p in probs]
     assert min(sizes) >= 16 * 16 and max(sizes) <= 256 * 256
     assert sizes == [p.num_elements for p in M.batch_config4()]
+
+
+def test_step_cost_model_prefers_what_the_kernels_reward():
+    """The autotuner's step model: a longer factor row costs quadratically
+    in the factorization, more levels cost in every GMRES step, and levels
+    big enough for two CTAs are cheaper per block."""
+    from gpu_fem_b200.batch import step_cost_us
+    n = 20000
+    short = step_cost_us(n, {"levels_L": 1000, "levels_U": 1000, "nnzb": 20 * n}, 50)
+    long_rows = step_cost_us(n, {"levels_L": 1000, "levels_U": 1000, "nnzb": 40 * n}, 50)
+    assert long_rows > short
+    deeper = step_cost_us(n, {"levels_L": 2000, "levels_U": 2000, "nnzb": 20 * n}, 50)
+    assert deeper > short
+    more_its = step_cost_us(n, {"levels_L": 1000, "levels_U": 1000, "nnzb": 20 * n}, 100)
+    assert more_its > short
+    # per level: one CTA below ~200 blocks, two above (cheaper per block)
+    one = step_cost_us(n, {"levels_L": 100, "levels_U": 100, "nnzb": n + 2 * 100 * 190}, 10)
+    two = step_cost_us(n, {"levels_L": 100, "levels_U": 100, "nnzb": n + 2 * 100 * 400}, 10)
+    assert two < 2 * one
