@@ -62,7 +62,7 @@ def test_ilu_factor_and_apply_match_oracle(oracle, fill):
     assert st == 0
     # Block ILU on these shells is numerically unstable (factor growth
     # ~1e13), so two correct factorizations that round in a different order
-    # differ entrywise far above machine precision. Parity is judged by what
+    # differ entrywise far above machine precision. Parity is measured by what
     # ILU(k) defines: (L U)_ij = A_ij on the pattern (backward error), for the
     # GPU factors (diagonal blocks hold U_ii^{-1}) and for the oracle's, plus
     # bitwise run-to-run equality.
