@@ -2,6 +2,7 @@
 // class and method names so driver code written against smdogroup/gpu_fem
 // ports with few edits:
 //   ElementAssembler      include/assembler.h:14-322
+//   BsrData (host copy)   include/linalg/bsr_utils.h:43-404
 //   BsrMat, createBsrMat  include/linalg/bsr_mat.h:9-357
 //   DeviceVec, HostVec    include/linalg/vec.h:146-371
 //   ILUk_Preconditioner   include/linalg/precond.h:5-55
@@ -33,6 +34,9 @@ inline void check(gf_status s, const char* where) {
 }
 
 template <typename T>
+class DeviceVec;
+
+template <typename T>
 class HostVec {
  public:
   HostVec() = default;
@@ -43,6 +47,11 @@ class HostVec {
   const T* getPtr() const { return v_.data(); }
   int getSize() const { return (int)v_.size(); }
   T& operator[](int i) { return v_[i]; }
+  const T& operator[](int i) const { return v_[i]; }
+  void zeroValues() { std::fill(v_.begin(), v_.end(), T(0)); }
+  void copyValuesTo(HostVec& o) const { std::copy(v_.begin(), v_.end(), o.getPtr()); }
+  // createDeviceVec (include/linalg/vec.h), defined after DeviceVec
+  DeviceVec<T> createDeviceVec() const;
 
  private:
   std::vector<T> v_;
@@ -76,6 +85,20 @@ class DeviceVec {
  private:
   int n_ = 0;
   std::shared_ptr<T> p_;
+};
+
+template <typename T>
+DeviceVec<T> HostVec<T>::createDeviceVec() const {
+  return DeviceVec<T>(*this);
+}
+
+// BsrData (include/linalg/bsr_utils.h:43-404): the block pattern in the
+// solver ordering with its permutation (perm[natural node] = solver row,
+// iperm its inverse) and elemIndMap (16 block slots per element). Host
+// copies; the device copies stay inside the library.
+struct BsrData {
+  int nnodes = 0, nnzb = 0;
+  HostVec<int> rowPtr, colPtr, perm, iperm, elemIndMap;
 };
 
 // ShellIsotropicData<double, has_ref_axis> (include/shell/data.h:8-47)
@@ -114,7 +137,35 @@ class ElementAssembler {
     gf_assembler* a = nullptr;
     check(gf_assembler_create(&d, &a), "gf_assembler_create");
     h_.reset(a, [](gf_assembler* x) { gf_assembler_destroy(x); });
+    xpts_ = xpts;
+    conn_ = geo_conn;
   }
+  // The pattern, ordering and elemIndMap are built by the constructor; the
+  // reference's symbolic_factorization(fill, print) (assembler.h:76-81)
+  // is kept for drivers that call it and changes nothing.
+  void symbolic_factorization(double fill = 100.0, bool print = false) {
+    (void)fill;
+    (void)print;
+  }
+  BsrData getBsrData() const {
+    BsrData b;
+    b.nnodes = get_num_nodes();
+    b.rowPtr = HostVec<int>(b.nnodes + 1);
+    check(gf_assembler_get_pattern(h_.get(), b.rowPtr.getPtr(), nullptr, nullptr, nullptr),
+          "getBsrData");
+    b.nnzb = b.rowPtr[b.nnodes];
+    b.colPtr = HostVec<int>(b.nnzb);
+    b.perm = HostVec<int>(b.nnodes);
+    b.iperm = HostVec<int>(b.nnodes);
+    b.elemIndMap = HostVec<int>(16 * get_num_elements());
+    check(gf_assembler_get_pattern(h_.get(), nullptr, b.colPtr.getPtr(), b.perm.getPtr(),
+                                   b.elemIndMap.getPtr()),
+          "getBsrData");
+    for (int i = 0; i < b.nnodes; i++) b.iperm[b.perm[i]] = i;
+    return b;
+  }
+  const HostVec<double>& getXpts() const { return xpts_; }
+  const HostVec<int>& getConn() const { return conn_; }
   int get_num_vars() const { return gf_assembler_num_vars(h_.get()); }
   int get_num_nodes() const { return gf_assembler_num_nodes(h_.get()); }
   int get_num_elements() const { return gf_assembler_num_elements(h_.get()); }
@@ -139,9 +190,17 @@ class ElementAssembler {
 
  private:
   std::shared_ptr<gf_assembler> h_;
+  HostVec<double> xpts_;
+  HostVec<int> conn_;
 };
 
 class BsrMat {
+  static int nnzb(const gf_assembler* a) {
+    std::vector<int> rp(gf_assembler_num_nodes(a) + 1);
+    check(gf_assembler_get_pattern(a, rp.data(), nullptr, nullptr, nullptr), "nnzb");
+    return rp.back();
+  }
+
  public:
   explicit BsrMat(ElementAssembler& a) : a_(a.handle()) {
     gf_bsr* m = nullptr;
@@ -150,6 +209,14 @@ class BsrMat {
   }
   double* getPtr() { return gf_bsr_values(h_.get()); }
   void zeroValues() { check(gf_bsr_zero(h_.get(), nullptr), "zeroValues"); }
+  // device-to-device copy of the 36 nnzb values into a matrix of the same pattern
+  void copyValuesTo(BsrMat& o) const {
+    if (o.a_ != a_) throw Error(GF_INVALID_ARG, "copyValuesTo");
+    const int nnzb = BsrMat::nnzb(a_);
+    if (cudaMemcpy(o.getPtr(), gf_bsr_values(h_.get()), sizeof(double) * 36 * (size_t)nnzb,
+                   cudaMemcpyDeviceToDevice) != cudaSuccess)
+      throw Error(GF_CUDA_ERROR, "copyValuesTo");
+  }
   gf_bsr* handle() const { return h_.get(); }
 
  private:
