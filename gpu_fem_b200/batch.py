@@ -29,7 +29,7 @@ import torch
 from . import _lib as L
 from .assembler import BsrMat, ElementAssembler, ILUk_Preconditioner, SolveOptions, _stream
 
-FILL_CANDIDATES = (0, 1, 2, 3, 4, 6, 8, 12, 16, 24)
+FILL_CANDIDATES = (0, 1, 2, 3, 4, 5, 6, 7, 8, 10, 12, 16, 24)
 
 
 class Batch:
