@@ -44,8 +44,19 @@ struct SweepCtl {
 };
 
 // ------------------------------------------------ barriers and bulk copies
-constexpr unsigned long long kWaitNs = 2000000000ull;  // bound of every device-side wait
+constexpr unsigned long long kWaitNs = 2000000000ull;  // default bound of every device-side wait
 constexpr int kSweepCta = 2;  // CTAs (one thread-block cluster) per problem for triangular work
+
+// Bound (ns) of the waits that end when a bulk copy lands or when the
+// partner CTA of a cluster arrives (gf_test_set_waits changes it). The waits
+// that drain a CTA's own copies in flight before it leaves always use kWaitNs.
+__device__ unsigned long long g_wait_ns = kWaitNs;
+// Failure-injection knob for tests (gf_test_set_waits): when non-zero, CTA
+// rank 1 of a split problem never arrives on its partner's meeting barriers,
+// so the partner's bounded wait runs out and the launch reports ST_TIMEOUT.
+// Every wait stays bounded and both CTAs still meet on the final cluster
+// barrier, so nothing hangs.
+__device__ int g_skip_meet = 0;
 
 __device__ __forceinline__ unsigned long long gtimer() {
   unsigned long long t;
@@ -74,12 +85,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
       : "memory");
   return ok != 0;
 }
-// bounded wait; returns false if kWaitNs passed first
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+// bounded wait; returns false if limit_ns passed first
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity,
+                                          unsigned long long limit_ns) {
   const unsigned long long t0 = gtimer();
   unsigned n = 0;
   while (!mbar_try_wait(bar, parity)) {
-    if ((++n & 255u) == 0u && gtimer() - t0 > kWaitNs) return false;
+    if ((++n & 255u) == 0u && gtimer() - t0 > limit_ns) return false;
   }
   return true;
 }
@@ -112,8 +124,9 @@ __device__ __forceinline__ void mbar_arrive_remote(unsigned addr) {
   asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(addr)
                : "memory");
 }
-// bounded wait with acquire at cluster scope; false if kWaitNs passed first
-__device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, unsigned parity) {
+// bounded wait with acquire at cluster scope; false if limit_ns passed first
+__device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, unsigned parity,
+                                                  unsigned long long limit_ns) {
   const unsigned long long t0 = gtimer();
   unsigned n = 0;
   while (true) {
@@ -125,7 +138,7 @@ __device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, unsigned parity
         : "r"(smem_u32(bar)), "r"(parity)
         : "memory");
     if (ok) return true;
-    if ((++n & 255u) == 0u && gtimer() - t0 > kWaitNs) return false;
+    if ((++n & 255u) == 0u && gtimer() - t0 > limit_ns) return false;
   }
 }
 // all threads of all CTAs of the cluster
@@ -277,6 +290,8 @@ __global__ void __launch_bounds__(kFacWarps * 32) bfactor_kernel(const ProbDev* 
   else
     __syncthreads();
   const unsigned pfbar = split ? cluster_map(smem_u32(fbar), rank ^ 1u) : 0u;
+  const unsigned long long wlim = g_wait_ns;
+  const bool arrive = !(g_skip_meet && rank == 1);
   const int wbase = split ? (int)rank * nw + warp : warp, wstride = split ? 2 * nw : nw;
   const int32_t* rowp = d.prowp;
   const int32_t* cols = d.pcols;
@@ -382,8 +397,8 @@ __global__ void __launch_bounds__(kFacWarps * 32) bfactor_kernel(const ProbDev* 
       // both CTAs' rows of this level are final before either starts the next
       if (threadIdx.x == 0) {
         const unsigned slot = (unsigned)(lev & 1);
-        mbar_arrive_remote(pfbar + 8u * slot);
-        if (!mbar_wait_cluster(&fbar[slot], (unsigned)((lev >> 1) & 1))) {
+        if (arrive) mbar_arrive_remote(pfbar + 8u * slot);
+        if (!mbar_wait_cluster(&fbar[slot], (unsigned)((lev >> 1) & 1), wlim)) {
           fabort = 1;
           atomicOr(&ctl->status, ST_TIMEOUT);
         }
@@ -508,6 +523,8 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
   const unsigned pring = cluster_map(smem_u32(ring), partner);
   const unsigned pxbar = cluster_map(smem_u32(xbar), partner);
   const int64_t* offs = T.off + (size_t)rank * (T.nch + 1);  // this CTA's half chunks
+  const unsigned long long wlim = g_wait_ns;
+  const bool arrive = !(g_skip_meet && rank == 1);
   const double* rb = rhs + 6 * (size_t)d.off;
   double* ob = out + 6 * (size_t)d.off;
   if (tid == 0) {
@@ -539,7 +556,7 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
     for (int c = 0; c < kStages - 1 && c < T.nch; c++) issue(c);
   int issued = min(kStages - 1, T.nch);
   // chunk 0 has no earlier rows: only its right-hand sides
-  if (!mbar_wait(&bar[0], 0u)) abort_flag = 1;
+  if (!mbar_wait(&bar[0], 0u, wlim)) abort_flag = 1;
   __syncthreads();
   // 6-double rows of x and of the right-hand side move as three 16-byte
   // pieces when both vectors are 16-byte aligned, else as six 8-byte ones
@@ -571,7 +588,7 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
   int c = 0;
   for (; c < T.nch; c++) {
     const int s = c % kStages;
-    if (c > 0 && !mbar_wait(&bar[s], (unsigned)((c / kStages) & 1))) abort_flag = 1;
+    if (c > 0 && !mbar_wait(&bar[s], (unsigned)((c / kStages) & 1), wlim)) abort_flag = 1;
     cp_async_wait_all();  // this thread's copies for chunk c have landed
     __syncthreads();      // this CTA's half of chunk c-1 solved; its stage and xbuf[(c+1)&1] are free
     if (c > 0 && split) {
@@ -579,8 +596,8 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
       // this CTA) is complete and visible once its arrival is seen
       if (tid == 0) {
         const unsigned slot = (unsigned)((c - 1) & 1);
-        mbar_arrive_remote(pxbar + 8u * slot);
-        if (!mbar_wait_cluster(&xbar[slot], (unsigned)(((c - 1) >> 1) & 1))) abort_flag = 1;
+        if (arrive) mbar_arrive_remote(pxbar + 8u * slot);
+        if (!mbar_wait_cluster(&xbar[slot], (unsigned)(((c - 1) >> 1) & 1), wlim)) abort_flag = 1;
       }
       __syncthreads();
     }
@@ -681,7 +698,8 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
   if (abort_flag && tid == producer) {
     atomicOr(&ctl->status, ST_TIMEOUT);
     // chunks c .. issued-1 may still be in flight: let them land (bounded)
-    for (int q = c; q < issued; q++) mbar_wait(&bar[q % kStages], (unsigned)((q / kStages) & 1));
+    for (int q = c; q < issued; q++)
+      mbar_wait(&bar[q % kStages], (unsigned)((q / kStages) & 1), kWaitNs);
   }
   // neither CTA leaves while the other may still write into its shared
   // memory; every path of both CTAs of a split problem reaches this point
@@ -1199,12 +1217,13 @@ static cudaError_t build_tri(gf_precond* p, const std::vector<int32_t>& diag, bo
       for (int k = 0; k < nb; k++) vpos[q + k] = v0 + 36 * (int64_t)k;
       q += nb;
     }
-  // algorithmic bytes of one sweep: per stored block its values, column
-  // index and the 6 x entries it multiplies; per row a row pointer, its
-  // right-hand side and its result
+  // algorithmic bytes of one sweep (compulsory unique traffic): per stored
+  // block its values and column index; per row a row pointer, its
+  // right-hand side and its result (each x entry is read once, however many
+  // blocks multiply it)
   gf_precond::Tri& t = p->tri[upper ? 1 : 0];
   t.nsplit = nsplit;
-  t.abytes = real * (36 * (long long)vs + 4 + 48) + (long long)n * (4 + 48 + 48);
+  t.abytes = real * (36 * (long long)vs + 4) + (long long)n * (4 + 48 + 48) + 4;
   t.nch = nch;
   t.stage = stage;
   t.capb = capb;
@@ -1256,6 +1275,11 @@ struct gf_batch {
 
 namespace gf {
 
+// two CTAs per level pay off once a level has more rows than one CTA's warps
+static int fac_split_of(const gf_precond* p) {
+  return p->pat.n > kFacWarps * std::max(p->nlevL, 1) ? 1 : 0;
+}
+
 static int sm_count() {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
@@ -1282,8 +1306,7 @@ static gf_status upload_desc(gf_batch* B) {
     d.pdiag = p->d_diag.p;
     d.LU64 = p->d_lu.p;
     d.nlevL = p->nlevL;
-    // two CTAs per level pay off once a level has more rows than one CTA's warps
-    d.fac_split = p->pat.n > 16 * std::max(p->nlevL, 1) ? 1 : 0;
+    d.fac_split = fac_split_of(p);
     d.nlevU = p->nlevU;
     d.levLptr = p->d_levLptr.p;
     d.levLrows = p->d_levLrows.p;
@@ -1488,9 +1511,27 @@ static gf_status bspmv(gf_batch* B, const int* live, const double* x, double alp
   return GF_OK;
 }
 
+// Reads and clears the status flags that the batch's kernels have recorded
+// since the last read (timeouts of bounded waits, zero pivots). Flags are
+// cleared only here, after they have been read, so a flag set by a launch
+// whose caller did not wait (gf_precond_apply) is reported by the next call
+// that reads them.
 static gf_status read_ctl(gf_batch* B, cudaStream_t st, SweepCtl* h) {
   GF_CUDA(cudaMemcpyAsync(h, B->d_ctl.p, sizeof(SweepCtl), cudaMemcpyDeviceToHost, st));
+  GF_CUDA(cudaMemsetAsync(B->d_ctl.p, 0, sizeof(SweepCtl), st));
   GF_CUDA(cudaStreamSynchronize(st));
+  return GF_OK;
+}
+static gf_status ctl_status(const SweepCtl& h) {
+  if (h.status & ST_TIMEOUT) {
+    set_last_error_text("a bounded device-side wait ran out (a stalled copy or partner CTA)");
+    return GF_TIMEOUT;
+  }
+  if (h.status & ST_ZERO_PIVOT) {
+    set_last_error_text("singular diagonal block in block row " + std::to_string(h.pivot - 1) +
+                        " (batch space)");
+    return GF_ZERO_PIVOT;
+  }
   return GF_OK;
 }
 
@@ -1504,7 +1545,6 @@ static gf_status batch_factor(gf_batch* B, cudaStream_t st) {
         p->a->pat.nnz(), p->d_amap.p, B->mats[k]->vals.p, p->d_lu.p); ::gf::count_launch();
   }
   GF_CHECK_LAUNCH();
-  GF_CUDA(cudaMemsetAsync(&B->d_ctl.p->status, 0, 2 * sizeof(int), st));
   {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(B->np * kSweepCta));
@@ -1542,9 +1582,7 @@ static gf_status batch_factor(gf_batch* B, cudaStream_t st) {
   SweepCtl h;
   gf_status s = read_ctl(B, st, &h);
   if (s != GF_OK) return s;
-  if (h.status & ST_TIMEOUT) return GF_TIMEOUT;
-  if (h.status & ST_ZERO_PIVOT) return GF_ZERO_PIVOT;
-  return GF_OK;
+  return ctl_status(h);
 }
 
 // Batched restarted GMRES on A x = b (batch space) for problems with
@@ -1574,6 +1612,7 @@ static gf_status bgmres(gf_batch* B, const double* b, double* x, int m, int max_
   for (int p = 0; p < np; p++)
     if (bn[p] == 0.0) bn[p] = 1.0;
   std::vector<int> live = live0, jc(np), runh(np);
+  SweepCtl ctlh{};
   std::vector<double> tf(np, 0.0);
   iters.assign(np, 0);
   restarts.assign(np, 0);
@@ -1658,7 +1697,11 @@ static gf_status bgmres(gf_batch* B, const double* b, double* x, int m, int max_
       }
       GF_CUDA(cudaMemcpyAsync(runh.data(), B->run.p, sizeof(int) * np, cudaMemcpyDeviceToHost,
                               st));
+      GF_CUDA(cudaMemcpyAsync(&ctlh, B->d_ctl.p, sizeof(SweepCtl), cudaMemcpyDeviceToHost, st));
       GF_CUDA(cudaStreamSynchronize(st));
+      // a sweep whose bounded wait ran out left a partial z: stop (the
+      // caller reads and clears the flag)
+      if (ctlh.status & ST_TIMEOUT) return GF_TIMEOUT;
       if (std::all_of(runh.begin(), runh.end(), [](int v) { return v == 0; })) break;
     }
     bbacksolve<<<pb, 128, 0, st>>>(np, m, G); ::gf::count_launch();
@@ -1919,6 +1962,34 @@ gf_status gf_precond_info(const gf_precond* p, int32_t* nnzb, int32_t* nl, int32
   return GF_OK;
 }
 
+gf_status gf_precond_layout(const gf_precond* p, int32_t* nsplit_L, int32_t* nsplit_U,
+                            int32_t* fac_split, int32_t* chunks_L, int32_t* chunks_U) {
+  if (!p) return GF_INVALID_ARG;
+  if (nsplit_L) *nsplit_L = p->tri[0].nsplit;
+  if (nsplit_U) *nsplit_U = p->tri[1].nsplit;
+  if (fac_split) *fac_split = fac_split_of(p);
+  if (chunks_L) *chunks_L = p->tri[0].nch;
+  if (chunks_U) *chunks_U = p->tri[1].nch;
+  return GF_OK;
+}
+
+gf_status gf_precond_status(gf_precond* p, void* stream) {
+  if (!p) return GF_INVALID_ARG;
+  if (!p->self) return GF_OK;  // nothing has run
+  SweepCtl h;
+  gf_status s = read_ctl(p->self, as_stream(stream), &h);
+  if (s != GF_OK) return s;
+  return ctl_status(h);
+}
+
+gf_status gf_test_set_waits(unsigned long long wait_ns, int32_t skip_meetings) {
+  const unsigned long long w = wait_ns ? wait_ns : kWaitNs;
+  const int k = skip_meetings ? 1 : 0;
+  GF_CUDA(cudaMemcpyToSymbol(g_wait_ns, &w, sizeof(w)));
+  GF_CUDA(cudaMemcpyToSymbol(g_skip_meet, &k, sizeof(k)));
+  return GF_OK;
+}
+
 gf_status gf_precond_get(const gf_precond* p, int32_t* rowPtr, int32_t* colPtr,
                          double* h_values) {
   if (!p) return GF_INVALID_ARG;
@@ -1968,7 +2039,12 @@ gf_status gf_precond_apply_noalloc(gf_precond* p, const double* d_r, double* d_z
   }
   int dev = 0;
   GF_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kNoAllocDevices) return GF_INVALID_ARG;
+  if (dev < 0 || dev >= kNoAllocDevices) {
+    set_last_error_text("gf_precond_apply_noalloc: device index " + std::to_string(dev) +
+                        " is above the " + std::to_string(kNoAllocDevices) +
+                        " devices this entry point supports");
+    return GF_INVALID_ARG;
+  }
   double* y = nullptr;
   {
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
@@ -1979,7 +2055,11 @@ gf_status gf_precond_apply_noalloc(gf_precond* p, const double* d_r, double* d_z
     }
     y = g_noalloc_ptr[dev];
   }
-  if (B->smemL > kSweepSmemMax || B->smemU > kSweepSmemMax) return GF_INVALID_ARG;
+  if (B->smemL > kSweepSmemMax || B->smemU > kSweepSmemMax) {
+    set_last_error_text("gf_precond_apply_noalloc: the sweeps need more shared memory than a "
+                        "CTA has");
+    return GF_INVALID_ARG;
+  }
   cudaStream_t st = as_stream(stream);
   // the same two sweep kernels as gf_precond_apply; y in the fixed array and
   // z written straight into d_z (a batch of one starts at offset 0)
@@ -2119,9 +2199,16 @@ gf_status gf_batch_solve(gf_batch* B, const double* const* d_b, double* const* d
   gf_status s = batch_solve_space(B, o, S, st);
   bpermute<<<grid, 256, 0, st>>>(B->d_perm_out.p, 1); ::gf::count_launch();
   GF_CHECK_LAUNCH();
-  GF_CUDA(cudaStreamSynchronize(st));
+  // every sweep of the solve has run: read and clear the device status
+  SweepCtl h;
+  gf_status sc = read_ctl(B, st, &h);
+  if (sc == GF_OK) sc = ctl_status(h);
+  if (sc != GF_OK) {
+    s = sc;
+    for (auto& x : S) x.status = sc;
+  }
   if (stats)
-    for (int k = 0; k < B->np; k++) stats[k] = S[k];
+    for (int k = 0; k < B->np && k < (int)S.size(); k++) stats[k] = S[k];
   return s;
 }
 

@@ -85,8 +85,9 @@ long long gf_launch_count(void);
 /* Sweep timing for benchmarks (no reference counterpart). While enabled,
  * the two triangular-sweep launches of every preconditioner apply are
  * bracketed by CUDA events on their stream, and the sweeps add their
- * algorithmic bytes (stored blocks: 36 values + column index + 6 gathered x
- * entries; rows: row pointer + right-hand side + result) to a device counter.
+ * algorithmic bytes (the compulsory unique traffic: stored blocks: 36 values
+ * + column index; rows: row pointer + right-hand side + result) to a device
+ * counter.
  * Enabling or disabling resets the totals. Meant for a benchmark driving
  * the library from one host thread. */
 gf_status gf_timing_enable(int32_t enable);
@@ -201,6 +202,25 @@ gf_status gf_precond_apply(gf_precond* p, const double* d_r, double* d_z, void* 
  * (different streams, no ordering between them) race on it. */
 #define GF_NOALLOC_MAX_DOUBLES 262144
 gf_status gf_precond_apply_noalloc(gf_precond* p, const double* d_r, double* d_z, void* stream);
+/* Reads and clears the status flags the preconditioner's kernels recorded
+ * since the last read: GF_TIMEOUT when a bounded device-side wait of a
+ * triangular sweep or of the factorization ran out (the apply's z is then
+ * incomplete), GF_ZERO_PIVOT for a singular diagonal block, else GF_OK.
+ * gf_precond_apply and gf_precond_apply_noalloc do not wait for the GPU, so
+ * their flags are reported here, or by the next gf_precond_factor /
+ * gf_gmres_solve on this preconditioner, which read and clear them too.
+ * Synchronises `stream`. No counterpart in the reference (which exits on
+ * errors, include/cuda_utils.h:35-43). */
+gf_status gf_precond_status(gf_precond* p, void* stream);
+/* How the triangular work of this preconditioner is laid out on the GPU:
+ * CTAs that share each sweep chunk's rows (1 or 2) for L and U, whether the
+ * factorization splits each level's rows over a 2-CTA cluster, and the
+ * number of chunks of each triangle (a chunk holds rows of one level; a
+ * level with more blocks than a chunk's stage spans several). Any pointer
+ * may be NULL. No reference counterpart (cuSPARSE's bsrsv2 level analysis is
+ * internal). */
+gf_status gf_precond_layout(const gf_precond* p, int32_t* nsplit_L, int32_t* nsplit_U,
+                            int32_t* fac_split, int32_t* chunks_L, int32_t* chunks_U);
 /* Pattern, level count and factor copy for checking. rowPtr/colPtr may be
  * NULL; values receives nnzb_pc*36 entries with the diagonal blocks holding
  * U_ii^{-1}. */
@@ -267,6 +287,19 @@ gf_status gf_batch_factor(gf_batch* b, void* stream);
  * d_x[k] is the initial guess); stats[k] per problem (may be NULL). */
 gf_status gf_batch_solve(gf_batch* b, const double* const* d_b, double* const* d_x,
                          const gf_solve_opts* opts, gf_solve_stats* stats, void* stream);
+
+/* ---- failure injection for tests ------------------------------------- */
+/* Sets, on the current device, the bound of the device-side waits that end
+ * when a bulk copy lands or a partner CTA arrives (wait_ns; 0 restores the
+ * default of 2 s), and whether CTA rank 1 of every split triangle or
+ * factorization skips its arrivals on the partner's meeting barriers
+ * (skip_meetings != 0), which makes the partner's bounded wait run out so
+ * that the launch reports GF_TIMEOUT. The waits that drain a CTA's own copies
+ * in flight keep the 2 s bound, and both CTAs of a cluster still meet on the
+ * final cluster barrier, so nothing hangs. Process-wide for the device: set
+ * it only while no other work of this library runs there, and restore it
+ * with gf_test_set_waits(0, 0). No reference counterpart. */
+gf_status gf_test_set_waits(unsigned long long wait_ns, int32_t skip_meetings);
 
 #ifdef __cplusplus
 }

@@ -19,6 +19,7 @@
 // (element chunks, chunk/element colouring, first-touch masks, level sets),
 // which the CUDA path must reproduce bit-exactly.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <complex>
 #include <cstdint>
@@ -434,6 +435,131 @@ void orc_ilu0_apply(int n, const int* rowp, const int* cols, const double* LU, c
   }
 }
 
+// z = U^{-1} L^{-1} r on factor values whose diagonal blocks hold U_ii^{-1}
+// (the layout the CUDA factorization produces): the same two block
+// triangular solves as orc_ilu0_apply, multiplying by the stored inverse
+// instead of inverting U_ii.
+void orc_ilu_apply_dinv(int n, const int* rowp, const int* cols, const double* LU,
+                        const double* r, double* z) {
+  std::vector<double> y((size_t)6 * n);
+  for (int i = 0; i < n; i++) {
+    double s[6];
+    for (int k = 0; k < 6; k++) s[k] = r[6 * (size_t)i + k];
+    for (int jp = rowp[i]; jp < rowp[i + 1] && cols[jp] < i; jp++) {
+      const double* B = &LU[36 * (size_t)jp];
+      const double* x = &y[6 * (size_t)cols[jp]];
+      for (int a = 0; a < 6; a++)
+        for (int b = 0; b < 6; b++) s[a] -= B[6 * a + b] * x[b];
+    }
+    for (int k = 0; k < 6; k++) y[6 * (size_t)i + k] = s[k];
+  }
+  for (int i = n - 1; i >= 0; i--) {
+    double s[6];
+    int dp = -1;
+    for (int k = 0; k < 6; k++) s[k] = y[6 * (size_t)i + k];
+    for (int jp = rowp[i]; jp < rowp[i + 1]; jp++) {
+      if (cols[jp] == i) dp = jp;
+      if (cols[jp] <= i) continue;
+      const double* B = &LU[36 * (size_t)jp];
+      const double* x = &z[6 * (size_t)cols[jp]];
+      for (int a = 0; a < 6; a++)
+        for (int b = 0; b < 6; b++) s[a] -= B[6 * a + b] * x[b];
+    }
+    const double* Di = &LU[36 * (size_t)dp];
+    for (int a = 0; a < 6; a++) {
+      double t = 0.0;
+      for (int b = 0; b < 6; b++) t += Di[6 * a + b] * s[b];
+      z[6 * (size_t)i + a] = t;
+    }
+  }
+}
+
+// Backward error of a block ILU factor on its own pattern, without forming
+// dense matrices: (L U)_ij = sum_{k <= min(i,j)} L_ik U_kj with L_ii = I,
+// compared with A_ij for every (i, j) of the pattern (ILU(k) is defined by
+// (L U)_ij = A_ij there). LU holds L below the diagonal, U above it and
+// U_ii^{-1} on it (the CUDA layout; dinv = 1) or U_ii (dinv = 0). A is
+// given on the same pattern. out[0] = max |(L U - A)_ij|, out[1] = max |A|.
+void orc_ilu_backward_error(int n, const int* rowp, const int* cols, const double* LU,
+                            const double* A, int dinv, double* out) {
+  std::vector<int> diag(n, -1);
+  for (int i = 0; i < n; i++)
+    for (int jp = rowp[i]; jp < rowp[i + 1]; jp++)
+      if (cols[jp] == i) diag[i] = jp;
+  std::vector<double> U((size_t)36 * n);  // U_ii
+  for (int i = 0; i < n; i++) {
+    const double* D = &LU[36 * (size_t)diag[i]];
+    if (dinv)
+      blk_inv6(D, &U[36 * (size_t)i]);
+    else
+      std::memcpy(&U[36 * (size_t)i], D, 36 * sizeof(double));
+  }
+  double emax = 0.0, amax = 0.0;
+#ifdef _OPENMP
+#pragma omp parallel reduction(max : emax, amax)
+#endif
+  {
+    std::vector<int> pos(n, -1);
+    std::vector<double> acc;
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 64)
+#endif
+    for (int i = 0; i < n; i++) {
+      const int r0 = rowp[i], r1 = rowp[i + 1];
+      acc.assign((size_t)36 * (r1 - r0), 0.0);
+      for (int jp = r0; jp < r1; jp++) pos[cols[jp]] = jp - r0;
+      auto add = [&](const double* Lik, int k) {  // acc[i, j] += L_ik U_kj, j in U(k)
+        for (int jp = diag[k]; jp < rowp[k + 1]; jp++) {
+          const int t = pos[cols[jp]];
+          if (t < 0) continue;
+          const double* Ukj = jp == diag[k] ? &U[36 * (size_t)k] : &LU[36 * (size_t)jp];
+          double* C = &acc[36 * (size_t)t];
+          if (!Lik) {
+            for (int q = 0; q < 36; q++) C[q] += Ukj[q];
+          } else {
+            for (int a = 0; a < 6; a++)
+              for (int b = 0; b < 6; b++) {
+                double sum = 0.0;
+                for (int m = 0; m < 6; m++) sum += Lik[6 * a + m] * Ukj[6 * m + b];
+                C[6 * a + b] += sum;
+              }
+          }
+        }
+      };
+      for (int kp = r0; kp < diag[i]; kp++) add(&LU[36 * (size_t)kp], cols[kp]);
+      add(nullptr, i);
+      for (int jp = r0; jp < r1; jp++) {
+        const double* a = &A[36 * (size_t)jp];
+        const double* c = &acc[36 * (size_t)(jp - r0)];
+        for (int q = 0; q < 36; q++) {
+          emax = std::max(emax, std::fabs(c[q] - a[q]));
+          amax = std::max(amax, std::fabs(a[q]));
+        }
+      }
+      for (int jp = r0; jp < r1; jp++) pos[cols[jp]] = -1;
+    }
+  }
+  out[0] = emax;
+  out[1] = amax;
+}
+
+// Copy A's blocks into a pattern that contains A's (copyValuesTo,
+// include/linalg/bsr_mat.h:145-193); other blocks of out are zeroed.
+// Returns 0, or 1 + the first row with a block missing from the pattern.
+int orc_scatter_to_pattern(int n, const int* rowp, const int* cols, const double* vals,
+                           const int* rowp2, const int* cols2, double* out) {
+  std::memset(out, 0, sizeof(double) * 36 * (size_t)rowp2[n]);
+  for (int i = 0; i < n; i++) {
+    int q = rowp2[i];
+    for (int jp = rowp[i]; jp < rowp[i + 1]; jp++) {
+      while (q < rowp2[i + 1] && cols2[q] < cols[jp]) q++;
+      if (q == rowp2[i + 1] || cols2[q] != cols[jp]) return i + 1;
+      std::memcpy(&out[36 * (size_t)q], &vals[36 * (size_t)jp], 36 * sizeof(double));
+    }
+  }
+  return 0;
+}
+
 // y = A x (BSR 6x6 row-major blocks)
 void orc_spmv(int n, const int* rowp, const int* cols, const double* A, const double* x,
               double* y) {
@@ -477,75 +603,103 @@ int orc_levels(int n, const int* rowp, const int* cols, int lower, int* level) {
 }
 
 // ------------------------------------------------------------- GMRES
-static double dotv(const std::vector<double>& a, const std::vector<double>& b) {
-  double s = 0.0;
-  for (size_t i = 0; i < a.size(); i++) s += a[i] * b[i];
-  return s;
-}
-
 // GMRES(m) with modified Gram-Schmidt and Givens rotations
 // (examples/iterative/gmres.cu:468-771; c = a/h, s = b/h as at :684-693),
-// restarted. side = 0: left preconditioning M^{-1} A x = M^{-1} b (the
-// reference's choice); side = 1: right preconditioning A M^{-1} y = b. The
-// inner loop stops when the Givens residual estimate reaches rtol times its
-// initial value; convergence is declared on the true relative residual
-// ||b - A x|| / ||b|| <= rtol, checked at every restart.
-int orc_gmres(int n, const int* rowp, const int* cols, const double* A, const double* LU,
-              const double* b, double* x, int m, double rtol, int maxit, int side, int* iters,
-              double* relres) {
-  size_t N = (size_t)6 * n;
+// restarted. A is on (rowp, cols); the block ILU factor LU is on its own
+// pattern (prowp, pcols) with U_ii^{-1} in its diagonal blocks. side = 0:
+// left preconditioning M^{-1} A x = M^{-1} b (the reference's choice);
+// side = 1: right preconditioning A M^{-1} y = b. The inner loop stops when
+// the Givens residual estimate reaches rtol times its initial value;
+// convergence is declared on the true relative residual ||b - A x|| / ||b||
+// <= rtol, checked at every restart. Vector work runs on nthreads threads.
+int orc_gmres_k(int n, const int* rowp, const int* cols, const double* A, const int* prowp,
+                const int* pcols, const double* LU, const double* b, double* x, int m,
+                double rtol, int maxit, int side, int nthreads, int* iters, double* relres) {
+  const size_t N = (size_t)6 * n;
+  const long long NN = (long long)N;
+  if (nthreads < 1) nthreads = 1;
   std::vector<std::vector<double>> V(m + 1, std::vector<double>(N));
   std::vector<double> H((size_t)(m + 1) * m), g(m + 1), cs(m), ss(m), w(N), t(N), r(N),
       bb(b, b + N), xx(x, x + N);
-  double bnorm = std::sqrt(dotv(bb, bb));
+  auto dot = [&](const std::vector<double>& a, const std::vector<double>& c) {
+    double s = 0.0;
+#ifdef _OPENMP
+#pragma omp parallel for reduction(+ : s) num_threads(nthreads) if (nthreads > 1)
+#endif
+    for (long long k = 0; k < NN; k++) s += a[k] * c[k];
+    return s;
+  };
+  auto axpy = [&](double a, const std::vector<double>& xv, std::vector<double>& yv) {
+#ifdef _OPENMP
+#pragma omp parallel for num_threads(nthreads) if (nthreads > 1)
+#endif
+    for (long long k = 0; k < NN; k++) yv[k] += a * xv[k];
+  };
+  auto spmv = [&](const double* in, double* out) {
+#ifdef _OPENMP
+#pragma omp parallel for num_threads(nthreads) schedule(static) if (nthreads > 1)
+#endif
+    for (int i = 0; i < n; i++) {
+      double s[6] = {0, 0, 0, 0, 0, 0};
+      for (int jp = rowp[i]; jp < rowp[i + 1]; jp++) {
+        const double* B = &A[36 * (size_t)jp];
+        const double* xv = &in[6 * (size_t)cols[jp]];
+        for (int a = 0; a < 6; a++)
+          for (int c = 0; c < 6; c++) s[a] += B[6 * a + c] * xv[c];
+      }
+      for (int a = 0; a < 6; a++) out[6 * (size_t)i + a] = s[a];
+    }
+  };
+  auto prec = [&](const double* in, double* out) {
+    orc_ilu_apply_dinv(n, prowp, pcols, LU, in, out);
+  };
+  double bnorm = std::sqrt(dot(bb, bb));
   if (bnorm == 0.0) bnorm = 1.0;
   int it = 0;
   auto true_res = [&]() {
-    orc_spmv(n, rowp, cols, A, xx.data(), t.data());
+    spmv(xx.data(), t.data());
     for (size_t i = 0; i < N; i++) r[i] = bb[i] - t[i];
-    return std::sqrt(dotv(r, r)) / bnorm;
+    return std::sqrt(dot(r, r)) / bnorm;
   };
   double rel = true_res();
   while (rel > rtol && it < maxit) {
-    // initial (preconditioned) residual
-    if (side == 0) {
-      orc_ilu0_apply(n, rowp, cols, LU, r.data(), V[0].data());
-    } else {
+    if (side == 0)
+      prec(r.data(), V[0].data());
+    else
       V[0] = r;
-    }
-    double beta = std::sqrt(dotv(V[0], V[0]));
-    if (beta == 0.0) break;
+    double beta = std::sqrt(dot(V[0], V[0]));
+    if (!(beta > 0.0) || !std::isfinite(beta)) break;
     for (size_t i = 0; i < N; i++) V[0][i] /= beta;
     std::fill(g.begin(), g.end(), 0.0);
     g[0] = beta;
-    double target = rtol * (side == 0 ? beta / rel : bnorm);
+    const double target = rtol * (side == 0 ? beta / rel : bnorm);
     int j = 0;
     for (; j < m && it < maxit; j++, it++) {
       if (side == 0) {
-        orc_spmv(n, rowp, cols, A, V[j].data(), t.data());
-        orc_ilu0_apply(n, rowp, cols, LU, t.data(), w.data());
+        spmv(V[j].data(), t.data());
+        prec(t.data(), w.data());
       } else {
-        orc_ilu0_apply(n, rowp, cols, LU, V[j].data(), t.data());
-        orc_spmv(n, rowp, cols, A, t.data(), w.data());
+        prec(V[j].data(), t.data());
+        spmv(t.data(), w.data());
       }
       for (int i = 0; i <= j; i++) {
-        double h = dotv(w, V[i]);
+        const double h = dot(w, V[i]);
         H[(size_t)i * m + j] = h;
-        for (size_t k = 0; k < N; k++) w[k] -= h * V[i][k];
+        axpy(-h, V[i], w);
       }
-      double hn = std::sqrt(dotv(w, w));
+      const double hn = std::sqrt(dot(w, w));
       H[(size_t)(j + 1) * m + j] = hn;
       if (hn != 0.0)
         for (size_t k = 0; k < N; k++) V[j + 1][k] = w[k] / hn;
       for (int i = 0; i < j; i++) {
-        double a = H[(size_t)i * m + j], c = H[(size_t)(i + 1) * m + j];
+        const double a = H[(size_t)i * m + j], c = H[(size_t)(i + 1) * m + j];
         H[(size_t)i * m + j] = cs[i] * a + ss[i] * c;
         H[(size_t)(i + 1) * m + j] = -ss[i] * a + cs[i] * c;
       }
-      double a = H[(size_t)j * m + j], c = H[(size_t)(j + 1) * m + j];
-      double hyp = std::sqrt(a * a + c * c);
-      cs[j] = a / hyp;
-      ss[j] = c / hyp;
+      const double a = H[(size_t)j * m + j], c = H[(size_t)(j + 1) * m + j];
+      const double hyp = std::sqrt(a * a + c * c);
+      cs[j] = hyp > 0.0 ? a / hyp : 1.0;
+      ss[j] = hyp > 0.0 ? c / hyp : 0.0;
       H[(size_t)j * m + j] = cs[j] * a + ss[j] * c;
       H[(size_t)(j + 1) * m + j] = 0.0;
       g[j + 1] = -ss[j] * g[j];
@@ -564,14 +718,14 @@ int orc_gmres(int n, const int* rowp, const int* cols, const double* A, const do
       y[i] = s / H[(size_t)i * m + i];
     }
     std::fill(w.begin(), w.end(), 0.0);
-    for (int i = 0; i < j; i++)
-      for (size_t k = 0; k < N; k++) w[k] += y[i] * V[i][k];
+    for (int i = 0; i < j; i++) axpy(y[i], V[i], w);
     if (side == 1) {
-      orc_ilu0_apply(n, rowp, cols, LU, w.data(), t.data());
-      w = t;
+      prec(w.data(), t.data());
+      w.swap(t);
     }
     for (size_t k = 0; k < N; k++) xx[k] += w[k];
     rel = true_res();
+    if (!std::isfinite(rel)) break;
   }
   for (size_t i = 0; i < N; i++) x[i] = xx[i];
   *iters = it;
@@ -653,5 +807,91 @@ int orc_iluk_pattern(int n, const int* rowp, const int* cols, int levFill, int* 
   if (cols_out)
     for (size_t k = 0; k < cl.size(); k++) cols_out[k] = cl[k];
   return (int)cl.size();
+}
+
+// The same Dirichlet elimination as orc_apply_bcs_mat in one pass over the
+// blocks, with a per-DOF mask instead of a scan of every block per BC DOF
+// (identical values: every entry of a BC row or column is assigned 0 or 1).
+void orc_apply_bcs_mat_fast(int nnodes, const int* rowp, const int* cols, const int* perm,
+                            int nbcs, const int* bcs, double* values) {
+  std::vector<unsigned char> mask(nnodes, 0);  // solver-order node -> constrained DOF bits
+  for (int ib = 0; ib < nbcs; ib++) mask[perm[bcs[ib] / 6]] |= (unsigned char)(1u << (bcs[ib] % 6));
+  for (int i = 0; i < nnodes; i++)
+    for (int jp = rowp[i]; jp < rowp[i + 1]; jp++) {
+      const int j = cols[jp];
+      if (!mask[i] && !mask[j]) continue;
+      double* v = &values[36 * (size_t)jp];
+      for (int r = 0; r < 6; r++)
+        for (int c = 0; c < 6; c++)
+          if (((mask[i] >> r) & 1) || ((mask[j] >> c) & 1))
+            v[6 * r + c] = (i == j && r == c) ? 1.0 : 0.0;
+    }
+}
+
+// One CPU solve of a shell problem along the path the GPU runs, for the
+// timed CPU baseline: block pattern (get_row_col_ptrs) in the given node
+// ordering (perm[old] = new), element assembly of K (add_jacobian_cpu,
+// elements on nthreads threads) and the Dirichlet elimination, symbolic
+// ILU(fill) (computeILUk), numeric block ILU, and right-preconditioned
+// GMRES(restart) to ||b - A x|| / ||b|| <= rtol (examples/iterative/gmres.cu
+// steps, FP64 throughout). x_out gets the displacements in natural order.
+// t[0..3]: seconds of pattern + symbolic ILU (set-up the GPU path keeps
+// resident between steps), assembly + BCs, numeric factorization, GMRES.
+// Returns 0 when converged, 1 when not, 2 on a singular pivot.
+int orc_solve_problem(int nelem, int nnodes, const int* conn, const double* xpts,
+                      const ShellData* data, int nbcs, const int* bcs, const double* loads,
+                      const int* perm, int fill, int restart, double rtol, int maxit,
+                      int nthreads, double* x_out, int* iters, double* relres, double* t) {
+  using clk = std::chrono::steady_clock;
+  auto sec = [](clk::time_point a, clk::time_point b) {
+    return std::chrono::duration<double>(b - a).count();
+  };
+  const auto t0 = clk::now();
+  const int nnz0 = orc_bsr_pattern(nelem, nnodes, conn, nullptr, nullptr);
+  std::vector<int> rowp0(nnodes + 1), cols0(nnz0), rowp(nnodes + 1), cols(nnz0),
+      emap((size_t)16 * nelem);
+  orc_bsr_pattern(nelem, nnodes, conn, rowp0.data(), cols0.data());
+  orc_permute_pattern(nnodes, rowp0.data(), cols0.data(), perm, rowp.data(), cols.data());
+  orc_elem_ind_map(nelem, conn, rowp.data(), cols.data(), perm, emap.data());
+  std::vector<int> prowp(nnodes + 1);
+  const int nnzp = orc_iluk_pattern(nnodes, rowp.data(), cols.data(), fill, prowp.data(), nullptr);
+  std::vector<int> pcols(nnzp);
+  orc_iluk_pattern(nnodes, rowp.data(), cols.data(), fill, prowp.data(), pcols.data());
+  const auto t1 = clk::now();
+  std::vector<double> A((size_t)36 * nnz0, 0.0);
+  orc_assemble_jacobian(nelem, conn, xpts, nullptr, data, emap.data(), A.data(), nullptr,
+                        nthreads);
+  orc_apply_bcs_mat_fast(nnodes, rowp.data(), cols.data(), perm, nbcs, bcs, A.data());
+  const auto t2 = clk::now();
+  std::vector<double> LU((size_t)36 * nnzp);
+  orc_scatter_to_pattern(nnodes, rowp.data(), cols.data(), A.data(), prowp.data(), pcols.data(),
+                         LU.data());
+  const int piv = orc_ilu0_factor(nnodes, prowp.data(), pcols.data(), LU.data());
+  if (piv) return 2;
+  for (int i = 0; i < nnodes; i++)
+    for (int jp = prowp[i]; jp < prowp[i + 1]; jp++)
+      if (pcols[jp] == i) {
+        double Di[36];
+        blk_inv6(&LU[36 * (size_t)jp], Di);
+        std::memcpy(&LU[36 * (size_t)jp], Di, sizeof(Di));
+      }
+  const auto t3 = clk::now();
+  const size_t N = (size_t)6 * nnodes;
+  std::vector<double> b(N), x(N, 0.0);
+  for (int i = 0; i < nnodes; i++)
+    for (int k = 0; k < 6; k++) b[6 * (size_t)perm[i] + k] = loads[6 * (size_t)i + k];
+  const int st = orc_gmres_k(nnodes, rowp.data(), cols.data(), A.data(), prowp.data(),
+                             pcols.data(), LU.data(), b.data(), x.data(), restart, rtol, maxit, 1,
+                             nthreads, iters, relres);
+  const auto t4 = clk::now();
+  for (int i = 0; i < nnodes; i++)
+    for (int k = 0; k < 6; k++) x_out[6 * (size_t)i + k] = x[6 * (size_t)perm[i] + k];
+  if (t) {
+    t[0] = sec(t0, t1);
+    t[1] = sec(t1, t2);
+    t[2] = sec(t2, t3);
+    t[3] = sec(t3, t4);
+  }
+  return st;
 }
 }  // extern "C"

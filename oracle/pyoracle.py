@@ -170,11 +170,12 @@ def assemble_residual(mesh, vars_):
     return res
 
 
-def apply_bcs_mat(rowp, cols, vals, perm, bcs):
+def apply_bcs_mat(rowp, cols, vals, perm, bcs, fast=False):
     n = len(rowp) - 1
     bcs = np.ascontiguousarray(bcs, np.int32)
     perm = np.ascontiguousarray(perm, np.int32)
-    lib().orc_apply_bcs_mat(n, _pi(rowp), _pi(cols), _pi(perm), len(bcs), _pi(bcs), _p(vals))
+    f = lib().orc_apply_bcs_mat_fast if fast else lib().orc_apply_bcs_mat
+    f(n, _pi(rowp), _pi(cols), _pi(perm), len(bcs), _pi(bcs), _p(vals))
 
 
 def full_fill_count(rowp, cols):
@@ -206,12 +207,52 @@ def levels(rowp, cols, lower=True):
     return nl, lv
 
 
-def gmres(rowp, cols, A, LU, b, m=50, rtol=1e-10, maxit=20000, side=0, x0=None):
-    x = np.zeros_like(b) if x0 is None else x0.copy()
+def invert_diag(rowp, cols, LU):
+    """Factor values with each diagonal block U_ii replaced by U_ii^-1."""
+    out = np.array(LU, np.float64).reshape(-1, 6, 6)
+    n = len(rowp) - 1
+    rows = np.repeat(np.arange(n), np.diff(rowp))
+    d = np.nonzero(cols == rows)[0]
+    out[d] = np.linalg.inv(out[d])
+    return out.ravel()
+
+
+def gmres(rowp, cols, A, LU, b, m=50, rtol=1e-10, maxit=20000, side=0, x0=None, prowp=None,
+          pcols=None, nthreads=1):
+    """Restarted GMRES(m) on A (rowp, cols) with the block ILU factor LU (as
+    returned by ilu0: U_ii on the diagonal) on its pattern (prowp, pcols;
+    A's pattern when omitted)."""
+    prowp = rowp if prowp is None else prowp
+    pcols = cols if pcols is None else pcols
+    LUd = invert_diag(prowp, pcols, LU)
+    b = np.ascontiguousarray(b, np.float64)
+    A = np.ascontiguousarray(A, np.float64)
+    x = np.zeros_like(b) if x0 is None else np.array(x0, np.float64)
     it, rel = C.c_int(), C.c_double()
-    st = lib().orc_gmres(len(rowp) - 1, _pi(rowp), _pi(cols), _p(A), _p(LU), _p(b), _p(x), m,
-                         C.c_double(rtol), maxit, side, C.byref(it), C.byref(rel))
+    st = lib().orc_gmres_k(len(rowp) - 1, _pi(rowp), _pi(cols), _p(A), _pi(prowp), _pi(pcols),
+                           _p(LUd), _p(b), _p(x), m, C.c_double(rtol), maxit, side, nthreads,
+                           C.byref(it), C.byref(rel))
     return st, x, it.value, rel.value
+
+
+def solve_problem(mesh, perm, fill, restart=200, rtol=1e-8, maxit=20000, nthreads=1):
+    """One compiled CPU solve of a shell mesh (pattern, assembly + BCs, ILU(fill),
+    right-preconditioned GMRES). Returns (status, x natural order, iterations,
+    relative residual, [setup, assembly, factor, gmres] seconds)."""
+    conn = np.ascontiguousarray(mesh.conn, np.int32)
+    xpts = np.ascontiguousarray(mesh.xpts, np.float64)
+    bcs = np.ascontiguousarray(mesh.bcs, np.int32)
+    loads = np.ascontiguousarray(mesh.loads, np.float64)
+    perm = np.ascontiguousarray(perm, np.int32)
+    data = data_array(mesh.E, mesh.nu, mesh.thick)
+    x = np.zeros(6 * mesh.num_nodes)
+    t = np.zeros(4)
+    it, rel = C.c_int(), C.c_double()
+    st = lib().orc_solve_problem(conn.shape[0], mesh.num_nodes, _pi(conn), _p(xpts), data,
+                                 len(bcs), _pi(bcs), _p(loads), _pi(perm), fill, restart,
+                                 C.c_double(rtol), maxit, nthreads, _p(x), C.byref(it),
+                                 C.byref(rel), _p(t))
+    return st, x, it.value, rel.value, t
 
 
 def dense_solve(A, b):
@@ -246,11 +287,28 @@ def iluk_pattern(rowp, cols, lev):
 def scatter_to_pattern(rowp, cols, vals, rowp2, cols2):
     """Copy A's blocks into a superset pattern (copyValuesTo, bsr_mat.h:145-193)."""
     out = np.zeros(36 * len(cols2))
-    V = vals.reshape(-1, 36)
-    O = out.reshape(-1, 36)
-    n = len(rowp) - 1
-    for i in range(n):
-        pos = {int(c): k for k, c in enumerate(cols2[rowp2[i]:rowp2[i + 1]], start=rowp2[i])}
-        for jp in range(rowp[i], rowp[i + 1]):
-            O[pos[int(cols[jp])]] = V[jp]
+    vals = np.ascontiguousarray(vals, np.float64)
+    st = lib().orc_scatter_to_pattern(len(rowp) - 1, _pi(rowp), _pi(cols), _p(vals), _pi(rowp2),
+                                      _pi(cols2), _p(out))
+    if st:
+        raise ValueError(f"row {st - 1} of A has a block outside the target pattern")
     return out
+
+
+def ilu_apply_dinv(rowp, cols, LU, r):
+    """z = U^-1 L^-1 r for factors whose diagonal blocks hold U_ii^-1."""
+    z = np.zeros_like(r)
+    LU = np.ascontiguousarray(LU, np.float64)
+    r = np.ascontiguousarray(r, np.float64)
+    lib().orc_ilu_apply_dinv(len(rowp) - 1, _pi(rowp), _pi(cols), _p(LU), _p(r), _p(z))
+    return z
+
+
+def ilu_backward_error(rowp, cols, LU, A, dinv=True):
+    """max |(L U - A)_ij| over the pattern and max |A| (sparse block products)."""
+    out = np.zeros(2)
+    LU = np.ascontiguousarray(LU, np.float64)
+    A = np.ascontiguousarray(A, np.float64)
+    lib().orc_ilu_backward_error(len(rowp) - 1, _pi(rowp), _pi(cols), _p(LU), _p(A),
+                                 1 if dinv else 0, _p(out))
+    return out[0], out[1]

@@ -1,6 +1,9 @@
 """Batched uneven solves: every problem's displacement matches a dense FP64
-solve, and is bitwise identical whether solved alone or inside the batch
-(FP64 and mixed precision)."""
+solve within 1e-8 relative, and is bitwise identical whether solved alone or
+inside the batch (FP64 and mixed precision). The solves run to a 1e-10
+relative residual, which these plates reach in FP64 (their rounding floor
+eps || |A| |x| || / ||b|| is 1e-12 to 7e-12), so the displacement check is
+not limited by the solver's stopping point."""
 import numpy as np
 import pytest
 
@@ -24,18 +27,19 @@ def test_batch_alone_equals_mix_and_matches_dense(oracle, mode):
     from gpu_fem_b200.assembler import ILUk_Preconditioner, gmres_solve
     from gpu_fem_b200.batch import BatchSolver, solve_opts
     meshes = _meshes()
-    bs = BatchSolver(meshes, fill=3)
+    rtol = 1e-10
+    bs = BatchSolver(meshes, fill=3, rtol=rtol)
     mixed, spmv32 = mode != "fp64", mode == "mixed_spmv32"
     stats = bs.step(mixed, spmv32=spmv32)
     x_mix = [x.cpu().numpy().copy() for x in bs.xs]
     for i, m in enumerate(meshes):
-        assert stats[i]["rel_residual"] <= 1e-8, stats[i]
+        assert stats[i]["rel_residual"] <= rtol, stats[i]
         # alone: the same problem through the single-problem entry point
         P = ILUk_Preconditioner(bs.asms[i], 3, "fp32" if mixed else "fp64")
         P.factor(bs.mats[i])
         x = torch.zeros_like(bs.bs[i])
         st, s1 = gmres_solve(bs.asms[i], bs.mats[i], P, bs.bs[i], x,
-                             solve_opts(1e-8, spmv32, bs.restart))
+                             solve_opts(rtol, spmv32, bs.restart))
         xa = x.cpu().numpy()
         assert np.array_equal(xa.view(np.uint64), x_mix[i].view(np.uint64)), (
             m.name, np.abs(xa - x_mix[i]).max())
@@ -48,7 +52,7 @@ def test_batch_alone_equals_mix_and_matches_dense(oracle, mode):
         xd = oracle.dense_solve(oracle.bsr_to_dense(rowp, cols, vals), b)
         xd = xd.reshape(-1, 6)[perm].ravel()
         err = np.linalg.norm(xa - xd) / np.linalg.norm(xd)
-        assert err <= 1e-6, (m.name, err)
+        assert err <= 1e-8, (m.name, err)
 
 
 def test_batch_autotuner_picks_converging_fill():

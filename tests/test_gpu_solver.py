@@ -142,12 +142,16 @@ def test_mixed_precision_refinement_reaches_fp64_tolerance(oracle):
         P = ILUk_Preconditioner(A, fill_level=3, precision=prec)
         P.factor(K)
         x = torch.zeros_like(b)
+        # solved to 1e-10 (this plate's FP64 rounding floor eps || |A| |x| ||
+        # / ||b|| is 5e-11)
+        # so that the displacement gate, 1e-8 relative to the dense FP64
+        # solve, does not depend on where the iteration stopped
         st, stats = gmres_solve(A, K, P, b, x, SolveOptions(restart=200, max_iters=4000,
-                                                            rtol=1e-8, mixed=mixed, side=1,
+                                                            rtol=1e-10, mixed=mixed, side=1,
                                                             inner_rtol=1e-3))
-        assert stats["rel_residual"] <= 1e-8, (mixed, stats)
+        assert stats["rel_residual"] <= 1e-10, (mixed, stats)
         err = np.linalg.norm(x.cpu().numpy() - x_dense) / np.linalg.norm(x_dense)
-        assert err <= 1e-6, (mixed, err, stats)
+        assert err <= 1e-8, (mixed, err, stats)
 
 
 def test_precond_apply_accepts_8_byte_aligned_vectors():

@@ -1,0 +1,79 @@
+"""Bounded device-side waits report GF_TIMEOUT and leave the context usable.
+
+The split factorization and the split sweeps meet the partner CTA of their
+cluster once per level / chunk on mbarriers with bounded waits. The test
+shortens the bound to 200 us and makes CTA rank 1 skip its meeting arrivals
+(gf_test_set_waits), so rank 0's wait runs out: the launch records a
+timeout, both CTAs still meet on the final cluster barrier, and the host
+reads GF_TIMEOUT from gf_precond_factor, gf_precond_status after an apply,
+and gf_gmres_solve. With the default bound restored, the same objects factor
+and solve correctly. No wait is removed, so nothing can hang, and nothing
+faults.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from gpu_fem_b200 import mesh as M
+
+pytestmark = pytest.mark.gpu
+
+
+def _status(P):
+    import torch
+    from gpu_fem_b200 import _lib as L
+    return L.lib().gf_precond_status(P.h, C.c_void_p(torch.cuda.current_stream().cuda_stream))
+
+
+def test_timeout_reported_and_context_usable():
+    import torch
+    from gpu_fem_b200 import _lib as L
+    from gpu_fem_b200.assembler import (ElementAssembler, ILUk_Preconditioner, SolveOptions,
+                                        createBsrMat, gmres_solve)
+    lib = L.lib()
+    mesh = M.plate(160, 80, 1.0, 0.5, lambda x, y: 0.002 + 0 * x, "all_edges",
+                   lambda q: 1e3 + 0 * q[:, 0])
+    A = ElementAssembler.from_mesh(mesh, ordering="natural")
+    K = createBsrMat(A)
+    A.add_jacobian(None, K, fuse_bcs=True)
+    P = ILUk_Preconditioner(A, fill_level=6, precision="fp64")
+    lay = [C.c_int32() for _ in range(5)]
+    L.check(lib.gf_precond_layout(P.h, *[C.byref(v) for v in lay]), "layout")
+    assert [v.value for v in lay[:3]] == [2, 2, 1]  # both sweeps and the factorization split
+    P.factor(K)
+    r = torch.tensor(np.random.default_rng(3).standard_normal(mesh.num_dof), device="cuda")
+    z_ok = torch.zeros_like(r)
+    P.apply(r, z_ok)
+    assert _status(P) == L.GF_OK
+    b = torch.tensor(mesh.loads, device="cuda")
+    opts = SolveOptions(restart=100, max_iters=3000, rtol=1e-8, side=1)
+    torch.cuda.synchronize()
+    try:
+        L.check(lib.gf_test_set_waits(200_000, 1), "set_waits")
+        # split factorization: the level meetings run out
+        with pytest.raises(L.GpuFemError) as err:
+            P.factor(K)
+        assert err.value.status == L.GF_TIMEOUT
+        # split sweeps: the chunk meetings run out; the apply itself does
+        # not wait for the GPU, the status query reports it
+        z = torch.zeros_like(r)
+        P.apply(r, z)
+        assert _status(P) == L.GF_TIMEOUT
+        assert _status(P) == L.GF_OK  # read and cleared
+        x = torch.zeros_like(b)
+        st, stats = gmres_solve(A, K, P, b, x, opts, raise_on_fail=False)
+        assert st == L.GF_TIMEOUT and stats["status"] == L.GF_TIMEOUT
+    finally:
+        L.check(lib.gf_test_set_waits(0, 0), "restore waits")
+    torch.cuda.synchronize()
+    # the context and the objects are still usable
+    P.factor(K)
+    z = torch.zeros_like(r)
+    P.apply(r, z)
+    assert _status(P) == L.GF_OK
+    torch.cuda.synchronize()
+    assert np.array_equal(z.cpu().numpy().view(np.uint64), z_ok.cpu().numpy().view(np.uint64))
+    x = torch.zeros_like(b)
+    st, stats = gmres_solve(A, K, P, b, x, opts)
+    assert st == L.GF_OK and stats["rel_residual"] <= 1e-8, stats

@@ -18,10 +18,10 @@ from gpu_fem_b200 import mesh as M
 pytestmark = pytest.mark.gpu
 
 
-def _factored(mesh, fill, precision):
+def _factored(mesh, fill, precision, ordering="rcm"):
     import torch
     from gpu_fem_b200.assembler import ElementAssembler, ILUk_Preconditioner, createBsrMat
-    A = ElementAssembler.from_mesh(mesh, ordering="rcm")
+    A = ElementAssembler.from_mesh(mesh, ordering=ordering)
     K = createBsrMat(A)
     A.add_jacobian(None, K, fuse_bcs=True)
     P = ILUk_Preconditioner(A, fill_level=fill, precision=precision)
@@ -30,13 +30,29 @@ def _factored(mesh, fill, precision):
     return A, K, P
 
 
+def _case(name):
+    """24x12 jittered cantilever, RCM, ILU(2): one CTA per sweep. 160x80
+    clamped plate, natural ordering, ILU(6), 13,041 nodes (below the array's
+    43,690-node capacity): both sweeps split every chunk over a 2-CTA
+    cluster, so the intermediate vector in the fixed array is written by two
+    CTAs and read back through the result ring."""
+    if name == "single_cta":
+        return M.plate_config2(24, 12), 2, "rcm", 1
+    return (M.plate(160, 80, 1.0, 0.5, lambda x, y: 0.002 + 0 * x, "all_edges",
+                    lambda q: 1e3 + 0 * q[:, 0]), 6, "natural", 2)
+
+
+@pytest.mark.parametrize("case", ["single_cta", "split"])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_noalloc_apply_matches_apply_twice(precision):
+def test_noalloc_apply_matches_apply_twice(precision, case):
     import torch
     from gpu_fem_b200 import _lib as L
     lib = L.lib()
-    mesh = M.plate_config2(24, 12)
-    A, K, P = _factored(mesh, 2, precision)
+    mesh, fill, ordering, nsplit = _case(case)
+    A, K, P = _factored(mesh, fill, precision, ordering)
+    ns = [C.c_int32(), C.c_int32()]
+    assert lib.gf_precond_layout(P.h, C.byref(ns[0]), C.byref(ns[1]), None, None, None) == L.GF_OK
+    assert (ns[0].value, ns[1].value) == (nsplit, nsplit)
     stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
     rng = np.random.default_rng(7)
     for call in range(2):
@@ -49,7 +65,7 @@ def test_noalloc_apply_matches_apply_twice(precision):
         st = lib.gf_precond_apply_noalloc(P.h, C.c_void_p(r.data_ptr()),
                                           C.c_void_p(z_new.data_ptr()), stream)
         assert st == L.GF_OK, L.lib().gf_last_error()
-        torch.cuda.synchronize()
+        assert lib.gf_precond_status(P.h, stream) == L.GF_OK  # no bounded wait ran out
         a, b = z_ref.cpu().numpy(), z_new.cpu().numpy()
         assert np.isfinite(b).all(), call
         assert np.abs(a - b).max() <= 1e-13 * np.abs(a).max(), (call, np.abs(a - b).max())
