@@ -4,15 +4,19 @@
 Workload: 64 independent clamped plates, element grids log-uniform 16^2 ..
 256^2 with aspect 1..4 (seed 4321), t ~ U(2, 8) mm, p ~ U(0.5, 2) kPa,
 E = 70 GPa, nu = 0.3. A step assembles the 6x6-block BSR Jacobian (fused
-BCs), factors the block ILU(k) preconditioner (k autotuned per problem) and
-solves every problem to ||b - A x|| / ||b|| <= 1e-8 with FP32 ILU + FP32
-SpMV inside FP64 GMRES / iterative refinement. `value` is whole-job solves/s
-with inputs resident in HBM; `e2e` repeats the step through the public API
-with the load vectors copied from pinned host memory and the displacements
-copied back inside the timed region. The FP64 GPU path is timed beside it.
+BCs), factors the block ILU(k) preconditioner (k per problem from the
+autotuner's table) and solves every problem to ||b - A x|| / ||b|| <= 1e-8
+with FP32 ILU factors inside FP64 GMRES, all 64 problems as one batch.
+`value` is whole-job solves/s with inputs resident in HBM; `e2e` repeats the
+step through the public API with the load vectors copied from pinned host
+memory and the displacements copied back inside the timed region. Beside
+it: the same batch with FP64 factors, the plain FP64 GPU path (each problem
+alone through gf_gmres_solve), the per-solve mixed-vs-FP64 displacement
+difference, the sweep kernel's roofline and a CPU baseline.
 
---impl reference times the CPU oracle (a restatement of the reference's CPU
-assembly plus FP64 ILU-GMRES) on a bounded sample of the same problems.
+--impl reference times the CPU path (the oracle's compiled restatement of
+the reference's CPU assembly plus FP64 block ILU(k) and GMRES, with the same
+fill and ordering) on a pool of single-threaded worker processes.
 
 Multi-GPU (torchrun): every rank solves its own full batch (replicas, weak
 scaling); the step time is the max over ranks.
@@ -44,6 +48,10 @@ def _args():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--problems", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true",
+                    help="skip the plain (one problem at a time) FP64 GPU path")
+    ap.add_argument("--tune", action="store_true",
+                    help="re-run the fill autotuner instead of the committed table")
     ap.add_argument("--serve-seconds", type=float, default=0.0,
                     help="length of the Poisson request stream of the serving run (0 skips it)")
     ap.add_argument("--assembly-case", action="store_true",
@@ -208,112 +216,110 @@ def _dist():
     return ws, rank, local
 
 
-def systematic_sample(meshes, offset, k=4):
-    """Indices of k problems spread evenly over the size ranking (ranks
-    offset, offset + n/k, ...): solves/s over such a sample estimates the
-    whole batch's solves/s without running every large problem on the CPU."""
-    order = sorted(range(len(meshes)), key=lambda i: meshes[i].num_elements)
-    stride = max(len(order) // k, 1)
-    return [order[(offset % stride) + j * stride] for j in range(k) if (offset % stride) + j * stride < len(order)]
+# DRAM bytes (read + write) of one launch of the sweep kernel on this
+# workload, from an ncu capture (profiles/); None until measured.
+SWEEP_TRAFFIC = None
+
+# Fill level k and node ordering of each of the 64 problems, as chosen by the
+# batch autotuner (gpu_fem_b200/batch.py: ordering by ILU(8) levels x blocks
+# per row, then the converging k of smallest modelled factor + solve time) on
+# a B200. Both arms run every problem with these, so their configs match;
+# `--tune` re-runs the autotuner and prints the table it finds.
+FILLS = None
+ORDERS = None  # one character per problem: "n" natural, "r" RCM
 
 
-def cpu_ordering(mesh, fill=8):
-    """The GPU path's ordering rule on the oracle: natural or RCM, whichever
-    gives fewer ILU(fill) levels x blocks per row."""
+def bench_config(meshes, fills, orders, ws):
+    """The workload description both arms print (identical for the same table)."""
+    return {"workload": WORKLOAD, "problems": len(meshes),
+            "dofs": int(sum(m.num_dof for m in meshes)),
+            "fill_levels": [int(k) for k in fills], "orderings": "".join(o[0] for o in orders),
+            "rtol": 1e-8, "gmres": "right-preconditioned GMRES(100), FP64 Krylov vectors",
+            "l2": "inputs larger than L2 (all 64 systems resident, ~GB)",
+            "parallelism": f"replicas x{ws}"}
+
+
+def table_or_none(n):
+    if FILLS is None or ORDERS is None or len(FILLS) != n or len(ORDERS) != n:
+        return None, None
+    return list(FILLS), ["natural" if c == "n" else "rcm" for c in ORDERS]
+
+
+# ---------------------------------------------------------------- CPU arm
+# The CPU path (the oracle's compiled restatement of the reference's CPU
+# assembly, add_jacobian_cpu, plus block ILU(k) and right-preconditioned
+# GMRES in FP64) runs one problem per process on a pool of single-threaded
+# workers (spawned, so no worker inherits a CUDA context): independent
+# problems are the CPU's natural parallelism, as they are the GPU batch's.
+_CPU = {}
+
+
+def _cpu_init(root, nprob):
+    sys.path.insert(0, root)
+    from gpu_fem_b200 import mesh as M
+    _CPU["meshes"] = M.batch_config4(nprob)
+
+
+def _cpu_solve(task):
+    """One problem: pattern, assembly + BCs, ILU(k), GMRES to 1e-8 (1 thread)."""
     import numpy as np
 
     from oracle import pyoracle as po
-    rowp0, cols0 = po.bsr_pattern(mesh.conn, mesh.num_nodes)
-    best = None
-    for name, perm in (("natural", np.arange(mesh.num_nodes, dtype=np.int32)),
-                       ("rcm", po.rcm(rowp0, cols0, 0, 1))):
-        rowp, cols = po.permute_pattern(rowp0, cols0, perm)
-        rk, ck = po.iluk_pattern(rowp, cols, fill)
-        nl, _ = po.levels(rk, ck, True)
-        nu, _ = po.levels(rk, ck, False)
-        score = (nl + nu) * len(ck) / mesh.num_nodes
-        if best is None or score < best[0]:
-            best = (score, name)
-    return best[1]
-
-
-def cpu_baseline_run(problems, fills, budget_s=25.0, threads=None, orders=None):
-    """Oracle (restated reference CPU path): assembly (OpenMP over elements),
-    FP64 block ILU(k), right-preconditioned GMRES, in the same ordering and
-    fill as the GPU path; on as many of the given problems as fit in about
-    budget_s. Returns (solves/s, n, seconds, cores)."""
-    import numpy as np
-
-    from oracle import pyoracle as po
-    threads = threads or os.cpu_count() or 1
-    orders = orders or ["rcm"] * len(problems)
-    t_total, n = 0.0, 0
-    for m, k, o in zip(problems, fills, orders):
-        t0 = time.perf_counter()
+    i, fill, order = task
+    m = _CPU["meshes"][i]
+    if order == "rcm":
         rowp0, cols0 = po.bsr_pattern(m.conn, m.num_nodes)
-        perm = (po.rcm(rowp0, cols0, 0, 1) if o == "rcm"
-                else np.arange(m.num_nodes, dtype=np.int32))
-        rowp, cols, A, _, perm = po.assemble_jacobian(m, perm=perm, nthreads=threads)
-        po.apply_bcs_mat(rowp, cols, A, perm, m.bcs)
-        b = np.zeros(6 * m.num_nodes)
-        b.reshape(-1, 6)[perm] = m.loads.reshape(-1, 6)
-        if k:
-            rk, ck = po.iluk_pattern(rowp, cols, k)
-            Ak = po.scatter_to_pattern(rowp, cols, A, rk, ck)
-        else:
-            rk, ck, Ak = rowp, cols, A
-        st, LU = po.ilu0(rk, ck, Ak)
-        # right preconditioning with the ILU(k) factors over A's pattern
-        st2, x, its, rel = _oracle_gmres_right(po, rowp, cols, A, rk, ck, LU, b)
-        dt = time.perf_counter() - t0
-        t_total += dt
-        n += 1
-        if t_total >= budget_s:
-            break
-    return n / t_total, n, t_total, threads
+        perm = po.rcm(rowp0, cols0, 0, 1)
+    else:
+        perm = np.arange(m.num_nodes, dtype=np.int32)
+    t0 = time.perf_counter()
+    st, x, it, rel, ph = po.solve_problem(m, perm, fill, restart=100, rtol=1e-8, maxit=20000,
+                                          nthreads=1)
+    # the timed CPU solve is assembly + factorization + GMRES; pattern, RCM
+    # and symbolic ILU are set-up kept between steps on both paths
+    return i, time.perf_counter() - t0 - ph[0], st, it, rel
 
 
-def _oracle_gmres_right(po, rowp, cols, A, rk, ck, LU, b, m=200, rtol=1e-8, maxit=5000):
-    """FP64 right-preconditioned GMRES(m) on the oracle kernels (numpy
-    Arnoldi, C SpMV and ILU apply)."""
-    import numpy as np
-    x = np.zeros_like(b)
-    bn = np.linalg.norm(b)
-    r = b - po.spmv(rowp, cols, A, x)
-    rel = np.linalg.norm(r) / bn
-    it = 0
-    while rel > rtol and it < maxit:
-        beta = np.linalg.norm(r)
-        V = [r / beta]
-        H = np.zeros((m + 1, m))
-        g = np.zeros(m + 1)
-        g[0] = beta
-        cs, ss = np.zeros(m), np.zeros(m)
-        j = 0
-        for j in range(m):
-            w = po.spmv(rowp, cols, A, po.ilu0_apply(rk, ck, LU, V[j]))
-            for i in range(j + 1):
-                H[i, j] = w @ V[i]
-                w = w - H[i, j] * V[i]
-            H[j + 1, j] = np.linalg.norm(w)
-            V.append(w / H[j + 1, j])
-            for i in range(j):
-                a, c = H[i, j], H[i + 1, j]
-                H[i, j], H[i + 1, j] = cs[i] * a + ss[i] * c, -ss[i] * a + cs[i] * c
-            a, c = H[j, j], H[j + 1, j]
-            h = np.hypot(a, c)
-            cs[j], ss[j] = a / h, c / h
-            H[j, j], H[j + 1, j] = cs[j] * a + ss[j] * c, 0.0
-            g[j + 1], g[j] = -ss[j] * g[j], cs[j] * g[j]
-            it += 1
-            if abs(g[j + 1]) <= rtol * bn:
-                break
-        jj = j + 1
-        y = np.linalg.solve(np.triu(H[:jj, :jj]), g[:jj])
-        x += po.ilu0_apply(rk, ck, LU, sum(y[i] * V[i] for i in range(jj)))
-        r = b - po.spmv(rowp, cols, A, x)
-        rel = np.linalg.norm(r) / bn
-    return (0 if rel <= rtol else 1), x, it, rel
+def cpu_groups(meshes, ngroups=4):
+    """Problems by size rank, dealt into ngroups groups (every ngroups-th),
+    so each group spans the whole size distribution."""
+    order = sorted(range(len(meshes)), key=lambda i: meshes[i].num_elements)
+    return [order[g::ngroups] for g in range(ngroups)]
+
+
+class CpuPool:
+    def __init__(self, nprob, cores=None):
+        import multiprocessing as mp
+        self.cores = cores or os.cpu_count() or 1
+        self.pool = mp.get_context("spawn").Pool(self.cores, initializer=_cpu_init,
+                                                 initargs=(ROOT, nprob))
+
+    def run(self, idx, fills, orders, meshes):
+        """Solve the problems idx, largest first; (wall s, sum of per-problem s)."""
+        tasks = sorted(((i, fills[i], orders[i]) for i in idx),
+                       key=lambda t: -meshes[t[0]].num_elements)
+        t0 = time.perf_counter()
+        out = list(self.pool.imap_unordered(_cpu_solve, tasks))
+        wall = time.perf_counter() - t0
+        bad = [o for o in out if o[2] != 0]
+        if bad:
+            raise RuntimeError(f"CPU solves did not converge: {bad[:3]}")
+        return wall, sum(o[1] for o in out)
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+
+def cpu_measure(meshes, fills, orders, groups, pool):
+    n = sum(len(g) for g in groups)
+    wall = ssum = 0.0
+    for g in groups:
+        w, t = pool.run(g, fills, orders, meshes)
+        wall += w
+        ssum += t
+    return {"all_core": n / wall, "single_thread": n / ssum, "n": n, "wall_s": wall,
+            "cores": pool.cores}
 
 
 def run_reference(args):
@@ -321,35 +327,70 @@ def run_reference(args):
     ws, rank, _ = _dist()
     if rank != 0:
         return
-    probs = M.batch_config4(args.problems)
-    vals = []
-    for s in range(args.warmup + args.steps):
-        idx = systematic_sample(probs, 2 + 5 * s)
-        sample = [probs[i] for i in idx]
-        v, n, sec, cores = cpu_baseline_run(sample, [_default_fill(p) for p in sample],
-                                            budget_s=1e9,
-                                            orders=[cpu_ordering(p) for p in sample])
-        if s >= args.warmup:
-            vals.append(v)
-    value = statistics.median(vals)
+    meshes = M.batch_config4(args.problems)
+    fills, orders = table_or_none(len(meshes))
+    if fills is None:
+        print(json.dumps({"impl": "reference", "unavailable": "no fill/ordering table for "
+                          "this problem count (run bench.py --tune on a GPU)"}), flush=True)
+        return
+    groups = cpu_groups(meshes)
+    pool = CpuPool(len(meshes))
+    try:
+        for s in range(args.warmup):
+            pool.run(groups[s % len(groups)], fills, orders, meshes)
+        per = [cpu_measure(meshes, fills, orders, [groups[(args.warmup + s) % len(groups)]], pool)
+               for s in range(args.steps)]
+    finally:
+        pool.close()
+    n = sum(p["n"] for p in per)
+    wall = sum(p["wall_s"] for p in per)
+    value = n / wall
+    single = n / sum(p["n"] / p["single_thread"] for p in per)
+    sample = (f"per step one group of {len(groups[0])} of the 64 problems (every 4th by size, "
+              f"groups in rotation), solved largest first on {pool.cores} single-threaded worker "
+              f"processes; each problem: assembly + BCs, ILU(k), right-preconditioned GMRES to "
+              f"1e-8 with the GPU path's fill and ordering; value = solves / wall time")
     line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * n / value,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * wall / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (seeded meshes)", "impl": "reference",
-            "config": {"workload": WORKLOAD,
-                       "sample": "4 problems per step spread over the size ranking"},
-            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port",
-                             "sample": "per step 4 of the 64 problems at size ranks o, o+16, "
-                                       "o+32, o+48 (o varies by step); ILU(8), same "
-                                       "ordering rule as the GPU path"},
+            "config": bench_config(meshes, fills, orders, ws),
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": pool.cores,
+                             "kind": "port", "sample": sample,
+                             "single_thread": {"value": single, "unit": "solves/s", "cores": 1}},
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-def _default_fill(mesh):
-    # offline sweep: thin, coarse plates need more fill (see DESIGN notes)
-    return 8
+def plain_fp64_run(bs):
+    """The plain FP64 GPU path: each problem alone through the single-problem
+    entry points (gf_add_jacobian with fused BCs, gf_precond_factor with FP64
+    factors, gf_gmres_solve), one after another on one stream. Returns ms for
+    all problems (one warm-up pass first)."""
+    import torch
+
+    from gpu_fem_b200.assembler import gmres_solve
+    from gpu_fem_b200.batch import solve_opts
+    opts = solve_opts(bs.rtol, False, bs.restart)
+
+    def one_pass():
+        for a, k, p, b, x in zip(bs.asms, bs.mats, bs.P64, bs.bs, bs.xs):
+            a.add_jacobian(None, k, fuse_bcs=True)
+            p.factor(k)
+            x.zero_()
+            st, stats = gmres_solve(a, k, p, b, x, opts)
+            if stats["rel_residual"] > bs.rtol:
+                raise RuntimeError(f"plain FP64 solve did not converge: {stats}")
+
+    one_pass()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    one_pass()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
 
 
 def main():
@@ -375,8 +416,12 @@ def main():
     from gpu_fem_b200.batch import BatchSolver
 
     meshes = M.batch_config4(args.problems)
+    fills, orders = table_or_none(len(meshes))
     t0 = time.perf_counter()
-    bs = BatchSolver(meshes, tune=True)
+    if fills is None or args.tune:
+        bs = BatchSolver(meshes, tune=True)
+    else:
+        bs = BatchSolver(meshes, ordering=orders, fill=fills, tune=False)
     setup_s = time.perf_counter() - t0
 
     def barrier():
@@ -442,6 +487,15 @@ def main():
     h2d = sum(8 * m.num_dof for m in meshes)
     nprob = len(meshes)
     value = job_throughput(nprob, ws, ms_mixed)
+    # per-solve displacement difference of the mixed path (FP32 factors)
+    # against the FP64 path, on the same problems
+    bs.step(True)
+    x_mixed = [x.cpu().numpy().copy() for x in bs.xs]
+    bs.step(False)
+    errs = [float(np.linalg.norm(a - x.cpu().numpy()) / np.linalg.norm(x.cpu().numpy()))
+            for a, x in zip(x_mixed, bs.xs)]
+    # the plain FP64 GPU path: one problem at a time (not batched)
+    ms_plain = None if args.no_plain else job_ms(plain_fp64_run(bs), ws, "cuda")
 
     # roofline of the dominant kernel, the block triangular sweeps
     # (bsweep_tma), from CUDA events around every sweep pair inside the timed
@@ -449,33 +503,34 @@ def main():
     peak, peak_kind = _peaks()
     sweep_s = sweep_ms / 1e3
     achieved = sweep_bytes / sweep_s / 1e9 if sweep_s > 0 else 0.0
-
+    orders_used = bs.orderings
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_mixed,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64 assembly, SpMV and GMRES; f32 ILU factor values", "data": "synthetic (seeded meshes)",
-        "config": {"workload": WORKLOAD, "problems": nprob,
-                   "dofs": int(sum(m.num_dof for m in meshes)),
-                   "fill_levels": bs.fills,
-                   "gmres_steps_max": {"mixed": its_mixed, "fp64": its_fp64},
-                   "l2": "inputs larger than L2 (all 64 systems resident, ~GB)",
-                   "setup_s": round(setup_s, 2), "parallelism": f"replicas x{ws}"},
+        "dtype": "f64 assembly, SpMV and GMRES; f32 ILU factor values",
+        "data": "synthetic (seeded meshes)",
+        "config": bench_config(meshes, bs.fills, orders_used, ws),
+        "setup_s": round(setup_s, 2),
+        "gmres_steps_max": {"mixed": its_mixed, "fp64": its_fp64},
         "latency_ms": {"p50": float(np.percentile(lat_mixed, 50)),
                        "p99": float(np.percentile(lat_mixed, 99)),
                        "note": "all 64 requests of a step complete together"},
         "fp64_gpu": {"value": job_throughput(nprob, ws, ms_fp64), "unit": "solves/s",
-                     "ms_per_step": ms_fp64,
+                     "ms_per_step": ms_fp64, "note": "the same batch with FP64 factors",
                      "latency_ms": {"p50": float(np.percentile(lat_fp64, 50)),
                                     "p99": float(np.percentile(lat_fp64, 99))}},
         "mixed_over_fp64": ms_fp64 / ms_mixed,
+        "mixed_vs_fp64_error": {"max": max(errs), "median": float(np.median(errs)),
+                                "per_solve": [float(f"{e:.3g}") for e in errs],
+                                "note": "||x_mixed - x_fp64|| / ||x_fp64|| per problem"},
         "phase_ms": {"assemble": phases_mixed[0], "factor": phases_mixed[1],
                      "solve": phases_mixed[2]},
         "e2e": {"value": job_throughput(nprob, ws, ms_e2e), "unit": "solves/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
         "roofline": {"kernel": "bsweep_tma (block L and U sweeps, FP32 factor values)",
                      "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": SWEEP_TRAFFIC,
                      "launches": sweep_launches,
                      "ms_per_launch": sweep_ms / max(sweep_launches, 1),
                      "algorithmic_bytes_per_launch": sweep_bytes / max(sweep_launches, 1),
@@ -483,16 +538,31 @@ def main():
         "clocks": clk,
         "gpu_launches": int(launches),
     }
+    if ms_plain is not None:
+        line["plain_fp64_gpu"] = {
+            "value": job_throughput(nprob, ws, ms_plain), "unit": "solves/s",
+            "ms_per_step": ms_plain,
+            "note": "each problem alone: gf_add_jacobian + gf_precond_factor (FP64 factors) + "
+                    "gf_gmres_solve, one after another"}
+        line["mixed_batched_over_plain_fp64"] = ms_plain / ms_mixed
+    if fills is None or args.tune:
+        line["tuned_table"] = {"fills": [int(k) for k in bs.fills],
+                               "orders": "".join(o[0] for o in bs.orderings)}
     if args.serve_seconds > 0:
         line["serving"] = serving_run(args.serve_seconds)
     if rank == 0 and not args.no_cpu_baseline and ws == 1:
-        idx = systematic_sample(meshes, 2)
-        v, n_cpu, sec, cores = cpu_baseline_run([meshes[i] for i in idx],
-                                                [bs.fills[i] for i in idx], budget_s=1e9,
-                                                orders=[bs.orderings[i] for i in idx])
-        line["cpu_baseline"] = {"value": v, "unit": "solves/s", "cores": cores, "kind": "port",
-                                "sample": f"{n_cpu} of the 64 problems at size ranks 2, 18, 34, "
-                                          f"50, same fill and ordering as the GPU ({sec:.1f} s)"}
+        pool = CpuPool(len(meshes))
+        try:
+            g = cpu_groups(meshes)
+            cb = cpu_measure(meshes, bs.fills, bs.orderings, [g[0]], pool)
+        finally:
+            pool.close()
+        line["cpu_baseline"] = {
+            "value": cb["all_core"], "unit": "solves/s", "cores": cb["cores"], "kind": "port",
+            "sample": f"{cb['n']} of the 64 problems (every 4th by size), solved largest first on "
+                      f"{cb['cores']} single-threaded worker processes with the GPU's fill and "
+                      f"ordering ({cb['wall_s']:.1f} s)",
+            "single_thread": {"value": cb["single_thread"], "unit": "solves/s", "cores": 1}}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if ws > 1:

@@ -137,9 +137,11 @@ class BatchSolver:
             picked = [choose_ordering(m) for m in meshes]
             self.orderings = [o for o, _ in picked]
             self.asms = [a for _, a in picked]
-        else:
-            self.orderings = [ordering] * len(meshes)
-            self.asms = [ElementAssembler.from_mesh(m, ordering=ordering) for m in meshes]
+        else:  # one ordering for all, or one per problem
+            self.orderings = ([ordering] * len(meshes) if isinstance(ordering, str)
+                              else list(ordering))
+            self.asms = [ElementAssembler.from_mesh(m, ordering=o)
+                         for m, o in zip(meshes, self.orderings)]
         self.mats = [BsrMat(a) for a in self.asms]
         self.bs = [torch.tensor(m.loads, device="cuda") for m in meshes]
         self.xs = [torch.zeros_like(b) for b in self.bs]
