@@ -14,8 +14,12 @@ membrane-dominated rows lose definiteness), so the fill level k of the
 symbolic ILU(k) (computeILUk, include/linalg/bsr_utils.h:678-807) is chosen
 per problem: every candidate k is tried on the whole batch in one batched
 solve (FP32 factors, the less forgiving precision, inside FP64 GMRES) with
-an iteration cap, and each problem keeps the converging k
-with the smallest modelled factor + solve time (step_cost_us).
+an iteration cap, and the converging candidates are combined so that the
+modelled time of the batched factor + solve is smallest (batch_cost_us):
+the batch runs as many GMRES steps as its slowest-converging problem needs
+and each launch lasts as long as its longest level chain, so a problem that
+converges early can take a lower fill (fewer levels, a cheaper
+factorization) at no cost in steps.
 The node ordering (natural or RCM) is chosen first, by levels x blocks per
 row of ILU(8).
 """
@@ -80,26 +84,83 @@ def solve_opts(rtol=1e-8, mixed=False, restart=100, max_iters=20000, inner_rtol=
 ORDERINGS = ("natural", "rcm")
 
 
-def step_cost_us(nrow, inf, iterations):
-    """Critical-path model of one factor + solve of a problem (microseconds),
+def factor_cost_us(nrow, inf):
+    """Critical path of one numeric factorization of a problem (microseconds),
     fitted to B200 runs of the 64-plate batch. The factorization walks its
     lower levels in rounds of one row per warp (16 warps, or 32 when levels
     average more than 16 rows and two CTAs share them); a row's steps are
     sequential and each updates about one row length of blocks, so a row
-    costs ~0.35 us x (lower blocks)^2. Every GMRES step runs both sweeps at
-    ~1.1 us a level plus ~9 ns per block of the level, or ~1.6 us plus
-    ~4.5 ns when levels average more than 200 blocks and two CTAs share
-    them, and ~150 us of SpMV, reductions and launches (in a batch every
-    step of the slowest-converging problem keeps all of them running)."""
-    lvl, lvu, nnzb = inf["levels_L"], inf["levels_U"], inf["nnzb"]
+    costs ~0.35 us x (lower blocks)^2."""
+    lvl, nnzb = inf["levels_L"], inf["nnzb"]
     lower = max(nnzb - nrow, 0) / (2.0 * nrow)
     rows_per_level = nrow / max(lvl, 1)
     warps = 32 if rows_per_level > 16 else 16
     rounds = max(1, -(-int(rows_per_level) // warps))
-    factor = lvl * rounds * 0.35 * lower * lower
-    blocks = max(nnzb - nrow, 0) / 2.0 / max(lvl, 1)
+    return lvl * rounds * 0.35 * lower * lower
+
+
+def sweep_cost_us(inf):
+    """Both triangular sweeps of one preconditioner apply (microseconds):
+    ~1.1 us a level plus ~9 ns per block of the level, or ~1.6 us plus
+    ~4.5 ns when levels average more than 200 blocks and two CTAs share
+    them."""
+    lvl, lvu, nnzb = inf["levels_L"], inf["levels_U"], inf["nnzb"]
+    nrow = inf.get("nrow")
+    blocks = max(nnzb - (nrow or 0), 0) / 2.0 / max(lvl, 1)
     per_level = 1.6 + 0.0045 * blocks if blocks > 200 else 1.1 + 0.009 * blocks
-    return factor + iterations * ((lvl + lvu) * per_level + 150.0)
+    return (lvl + lvu) * per_level
+
+
+STEP_OVERHEAD_US = 150.0  # SpMV, orthogonalisation and launches of one GMRES step
+
+
+def step_cost_us(nrow, inf, iterations):
+    """Factor + solve time of a problem alone (microseconds): the
+    factorization plus, per GMRES step, both sweeps and ~150 us of SpMV,
+    reductions and launches."""
+    inf = dict(inf, nrow=nrow)
+    return factor_cost_us(nrow, inf) + iterations * (sweep_cost_us(inf) + STEP_OVERHEAD_US)
+
+
+def batch_cost_us(choice):
+    """Modelled time of one batched factor + solve (microseconds). choice:
+    per problem (iterations, factor us, sweep us per GMRES step). The
+    factorization of a batch is one launch, so it costs its slowest
+    problem's; GMRES step s costs the slowest sweep among the problems still
+    iterating at s (a sweep launch lasts as long as its longest level chain)."""
+    fac = max(c[1] for c in choice)
+    total, run_max, prev = 0.0, 0.0, 0
+    # walk the steps from the last backwards: problems join the running set
+    # in order of decreasing iteration count
+    for its, _, sw in sorted(choice, key=lambda c: -c[0]):
+        if its < prev or prev == 0:
+            total += (prev - its) * (run_max + STEP_OVERHEAD_US) if prev else 0.0
+            prev = its
+        run_max = max(run_max, sw)
+    total += prev * (run_max + STEP_OVERHEAD_US)
+    return fac + total
+
+
+def choose_batch_fills(cands, rounds=8):
+    """Per-problem fill levels that minimise batch_cost_us. cands[p]: list of
+    (k, iterations, factor us, sweep us) of the converging candidates of
+    problem p. Starts from every problem's own cheapest candidate and
+    changes one problem at a time while the batch's modelled time drops."""
+    pick = [min(c, key=lambda t: t[2] + t[1] * (t[3] + STEP_OVERHEAD_US)) for c in cands]
+    best = batch_cost_us([p[1:] for p in pick])
+    for _ in range(rounds):
+        improved = False
+        for p in range(len(cands)):
+            for cand in cands[p]:
+                if cand is pick[p]:
+                    continue
+                trial = pick[:p] + [cand] + pick[p + 1:]
+                t = batch_cost_us([q[1:] for q in trial])
+                if t < best - 1e-9:
+                    best, pick, improved = t, trial, True
+        if not improved:
+            break
+    return [p[0] for p in pick], best
 
 
 def choose_ordering(mesh, fill=8):
@@ -130,8 +191,12 @@ class BatchSolver:
     """Problems resident on the current device, solved as one batch."""
 
     def __init__(self, meshes, ordering="auto", tune=True, fill=None, rtol=1e-8, restart=100,
-                 build=True):
+                 build=True, objective="batch"):
         self.rtol, self.restart = rtol, restart
+        # autotuner objective: "batch" minimises the modelled time of the
+        # batched factor + solve (batch_cost_us), "problem" each problem's
+        # own factor + solve time
+        self.objective = objective
         self.meshes = meshes
         if ordering == "auto":
             picked = [choose_ordering(m) for m in meshes]
@@ -166,6 +231,7 @@ class BatchSolver:
     def _autotune(self, cap=400):
         n = len(self.meshes)
         best = [None] * n
+        cands = [[] for _ in range(n)]
         log = []
         for k in FILL_CANDIDATES:
             todo = [i for i in range(n) if best[i] is None or k <= best[i][2] + 4]
@@ -188,12 +254,15 @@ class BatchSolver:
                                  solve_opts(self.rtol, False, restart=self.restart, max_iters=cap))
             for j, i in enumerate(todo):
                 s = stats[j]
-                inf = P[j].info()
+                nrow = self.asms[i].get_num_nodes()
+                inf = dict(P[j].info(), nrow=nrow)
                 nlev = inf["levels_L"] + inf["levels_U"]
                 ok = s["status"] == L.GF_OK
                 log.append((i, k, s["iterations"], s["rel_residual"], nlev, ok))
                 if ok:
-                    cost = step_cost_us(self.asms[i].get_num_nodes(), inf, s["iterations"])
+                    cands[i].append((k, s["iterations"], factor_cost_us(nrow, inf),
+                                     sweep_cost_us(inf)))
+                    cost = step_cost_us(nrow, inf, s["iterations"])
                     if best[i] is None or cost < best[i][0]:
                         best[i] = (cost, k, k)
             if all(b is not None for b in best) and k >= max(b[1] for b in best) + 4:
@@ -201,7 +270,10 @@ class BatchSolver:
         missing = [self.meshes[i].name for i in range(n) if best[i] is None]
         if missing:
             raise RuntimeError(f"no ILU fill level converged for {missing}")
-        return [b[1] for b in best], log
+        if self.objective == "problem":
+            return [b[1] for b in best], log
+        fills, _ = choose_batch_fills(cands)
+        return fills, log
 
     def step(self, mixed: bool, host_io=None, spmv32=False, phases=None):
         """Assemble, factor and solve every problem once. mixed: FP32 ILU

@@ -63,3 +63,23 @@ def test_step_cost_model_prefers_what_the_kernels_reward():
     one = step_cost_us(n, {"levels_L": 100, "levels_U": 100, "nnzb": n + 2 * 100 * 190}, 10)
     two = step_cost_us(n, {"levels_L": 100, "levels_U": 100, "nnzb": n + 2 * 100 * 400}, 10)
     assert two < 2 * one
+
+
+def test_batch_objective_lowers_fill_of_early_converging_problems():
+    """In a batch, GMRES runs as many steps as the slowest problem needs and
+    each launch lasts as long as its longest level chain: a problem that
+    converges early at high fill is better off at a lower fill with more
+    (but still fewer than the batch's) steps."""
+    from gpu_fem_b200.batch import batch_cost_us, choose_batch_fills
+    slow = [(5, 100, 1000.0, 500.0)]                       # (k, steps, factor us, sweep us)
+    fast = [(8, 10, 5000.0, 2000.0), (3, 60, 500.0, 600.0)]
+    # 1000 + 60 x (600 + 150) + 40 x (500 + 150)
+    assert batch_cost_us([(100, 1000.0, 500.0), (60, 500.0, 600.0)]) == 72000.0
+    # 5000 + 10 x (2000 + 150) + 90 x (500 + 150)
+    assert batch_cost_us([(100, 1000.0, 500.0), (10, 5000.0, 2000.0)]) == 85000.0
+    fills, cost = choose_batch_fills([slow, fast])
+    assert fills == [5, 3] and cost == 72000.0
+    # alone, the fast problem's own cheapest candidate is the high fill
+    from gpu_fem_b200.batch import STEP_OVERHEAD_US
+    own = min(fast, key=lambda t: t[2] + t[1] * (t[3] + STEP_OVERHEAD_US))
+    assert own[0] == 8
