@@ -17,6 +17,7 @@ GF_OK, GF_INVALID_ARG, GF_OOM, GF_ZERO_PIVOT, GF_NOT_CONVERGED, GF_NAN, GF_TIMEO
 GF_ORDER_NATURAL, GF_ORDER_RCM = 0, 1
 GF_ASSEMBLE_OVERWRITE, GF_ASSEMBLE_ADD, GF_ASSEMBLE_FUSE_BCS = 0, 1, 2
 GF_PREC_FP64, GF_PREC_FP32 = 0, 1
+GF_SWEEP_AUTO, GF_SWEEP_DATAFLOW, GF_SWEEP_LEVEL = 0, 1, 2
 
 
 class GpuFemError(RuntimeError):
@@ -89,6 +90,8 @@ SIGNATURES = {
     "gf_bsr_spmv": (_I, [_P, _D, _P, _D, _P, _P]),
     "gf_permute_vec": (_I, [_P, _P, _P, _I, _P]),
     "gf_precond_create": (_I, [_P, _I, _I, C.POINTER(_P)]),
+    "gf_precond_create_ex": (_I, [_P, _I, _I, _I, C.POINTER(_P)]),
+    "gf_precond_sweeps": (_I, [_P, _PI, _PI, _PI, _PI]),
     "gf_precond_destroy": (_I, [_P]),
     "gf_precond_factor": (_I, [_P, _P, _P]),
     "gf_precond_apply": (_I, [_P, _P, _P, _P]),

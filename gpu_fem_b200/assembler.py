@@ -266,11 +266,15 @@ class ILUk_Preconditioner:
     """ILUk_Preconditioner (include/linalg/precond.h:5-55) with computeILUk's
     symbolic fill (include/linalg/bsr_utils.h:678-807)."""
 
-    def __init__(self, assembler: ElementAssembler, fill_level=0, precision="fp64"):
+    def __init__(self, assembler: ElementAssembler, fill_level=0, precision="fp64",
+                 sweep="auto"):
+        """sweep: "auto", "dataflow" or "level" (gf_precond_create_ex)."""
         self.assembler = assembler
         h = C.c_void_p()
         prec = {"fp64": L.GF_PREC_FP64, "fp32": L.GF_PREC_FP32}[precision]
-        check(L.lib().gf_precond_create(assembler.h, fill_level, prec, C.byref(h)),
+        kind = {"auto": L.GF_SWEEP_AUTO, "dataflow": L.GF_SWEEP_DATAFLOW,
+                "level": L.GF_SWEEP_LEVEL}[sweep]
+        check(L.lib().gf_precond_create_ex(assembler.h, fill_level, prec, kind, C.byref(h)),
               "gf_precond_create")
         self.h = h
 
@@ -290,6 +294,25 @@ class ILUk_Preconditioner:
         a, b, c = C.c_int32(), C.c_int32(), C.c_int32()
         check(L.lib().gf_precond_info(self.h, C.byref(a), C.byref(b), C.byref(c)), "info")
         return {"nnzb": a.value, "levels_L": b.value, "levels_U": c.value}
+
+    def sweeps(self):
+        """Sweep kernel of the L and U triangles ("dataflow" / "level") and the
+        dataflow result rings' slots."""
+        v = [C.c_int32() for _ in range(4)]
+        check(L.lib().gf_precond_sweeps(self.h, *[C.byref(x) for x in v]), "sweeps")
+        name = {L.GF_SWEEP_DATAFLOW: "dataflow", L.GF_SWEEP_LEVEL: "level"}
+        return {"L": name[v[0].value], "U": name[v[1].value], "ring_L": v[2].value,
+                "ring_U": v[3].value}
+
+    def layout(self):
+        v = [C.c_int32() for _ in range(5)]
+        check(L.lib().gf_precond_layout(self.h, *[C.byref(x) for x in v]), "layout")
+        return {"nsplit_L": v[0].value, "nsplit_U": v[1].value, "fac_split": v[2].value,
+                "chunks_L": v[3].value, "chunks_U": v[4].value}
+
+    def status(self):
+        """gf_precond_status: reads and clears the device-side status flags."""
+        return L.lib().gf_precond_status(self.h, _stream())
 
     def get(self):
         inf = self.info()

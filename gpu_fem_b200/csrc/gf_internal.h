@@ -112,14 +112,30 @@ constexpr int kMaxEC = 15;
 // so one bulk copy brings everything a chunk's solve needs into shared
 // memory. nblocks is a non-zero multiple of 4 (zero padding blocks). For U
 // every row starts with its U_ii^{-1} block.
+//
+// A triangle solved by the dataflow sweep (kind TRI_DATAFLOW) has a simpler
+// stream: rows in level order (position p = 0..n-1) cut into chunks of
+// consecutive positions (at most capb blocks and capr rows), chunk c being
+//   int4 header {nrows, nblocks, first position, 0}
+//   nrows x int4 {row, first block (chunk-local), blocks, 0}
+//   nblocks x int32 position of the row each block multiplies (-1 for U's
+//     leading U_ii^{-1} block and for padding), ascending within a row
+//   (16-byte aligned) nblocks x 36 values
+// and a row's x entries come from a shared-memory ring of the latest `ring`
+// positions' results (ring > 2 maxdist, maxdist = the largest position
+// distance between a row and a row it multiplies).
+enum { TRI_LEVEL = 0, TRI_DATAFLOW = 1 };
 struct TriDesc {
   int nch;                       // chunks
   int stage;                     // bytes of the largest chunk (staging buffer size)
   int capb, capr;                // blocks / rows per chunk at most
-  const int64_t* off;            // [2 (nch+1)] byte offsets of the two halves' chunks
+  const int64_t* off;            // level: [2 (nch+1)] byte offsets of the two halves'
+                                 // chunks; dataflow: [nch+1]
   const unsigned char* stream;
   long long abytes;              // algorithmic bytes of one sweep (for timing)
-  int nsplit;                    // CTAs that share each chunk's rows (1 or 2)
+  int nsplit;                    // level: CTAs that share each chunk's rows (1 or 2)
+  int kind;                      // TRI_LEVEL or TRI_DATAFLOW
+  int ring, maxdist;             // dataflow: ring slots (a power of two), dependency reach
 };
 
 // Per-problem descriptor used by the batched solver kernels: block rows,

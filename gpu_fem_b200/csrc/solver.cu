@@ -508,6 +508,7 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
   const int p = blockIdx.x / kSweepCta;
   const unsigned rank = cluster_rank(), partner = rank ^ 1u;
   if (live && !live[p]) return;  // the same for every CTA of the cluster
+  if ((UPPER ? P[p].U.kind : P[p].L.kind) != TRI_LEVEL) return;  // solved by bsweep_df
   const bool split = (UPPER ? P[p].U.nsplit : P[p].L.nsplit) > 1;
   if (!split && rank != 0) return;  // one CTA solves the whole chunk; no cluster traffic
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
@@ -725,6 +726,219 @@ static cudaError_t launch_sweep(int np, size_t smem, cudaStream_t st, const Prob
   cfg.numAttrs = 1;
   ::gf::count_launch();
   return cudaLaunchKernelEx(&cfg, bsweep_tma<VT, UPPER>, desc, live, rhs, out, ctl, ctr);
+}
+
+// ------------------------------------------------------ dataflow sweeps
+// One CTA per problem walks one triangle row by row in level order without
+// block barriers: compute warp w solves the rows of every chunk whose
+// chunk-local index is w mod kDfWarps, and a row waits only for the rows it
+// multiplies. A solved row's x entries go to global memory (the result) and
+// to a shared-memory ring of the latest `ring` positions, tagged with the
+// position they hold; a consumer waits (bounded) until the tag of each slot
+// it reads shows the row it needs, with acquire / release ordering at CTA
+// scope. A row's blocks are ordered by the position they depend on, so the
+// lane groups multiply the long-solved rows while the latest ones finish.
+// Flow control keeps the ring safe: before overwriting a slot with position
+// p a warp waits until every warp has moved past p - ring + maxdist (so all
+// readers of the slot's previous position are done), using the positions
+// the warps publish in wpos[]. Every position below min(wpos) is solved, so
+// the warp holding that minimum can always proceed: nothing waits in a
+// cycle. The factor stream arrives through kDfStages shared-memory stages
+// filled by 1D bulk copies, which the last warp issues as the compute warps
+// release stages (a full / empty mbarrier pair per stage). All waits are
+// bounded; on a timeout the CTA records ST_TIMEOUT and ends after its copies
+// in flight have landed.
+constexpr int kDfThreads = 512;
+constexpr int kDfWarps = kDfThreads / 32 - 1;  // compute warps; the last warp issues copies
+constexpr int kDfStages = 4;
+
+// dynamic shared memory of a dataflow sweep: the stages, the ring's x entries
+// (6 doubles) and tags (int)
+__host__ __device__ inline size_t df_smem_bytes(int stage, int ring) {
+  return kDfStages * (size_t)stage + (size_t)ring * (48 + 4);
+}
+__device__ __forceinline__ void mbar_arrive_local(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ int ld_acquire_s32(const int* p) {
+  int v;
+  asm volatile("ld.acquire.cta.shared.b32 %0, [%1];" : "=r"(v) : "r"(smem_u32(p)) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_s32(int* p, int v) {
+  asm volatile("st.release.cta.shared.b32 [%0], %1;" ::"r"(smem_u32(p)), "r"(v) : "memory");
+}
+
+template <class VT, bool UPPER>
+__global__ void __launch_bounds__(kDfThreads) bsweep_df(const ProbDev* __restrict__ P,
+                                                       const int* __restrict__ live,
+                                                       const double* __restrict__ rhs,
+                                                       double* out, SweepCtl* ctl,
+                                                       unsigned long long* bytes_ctr) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ uint64_t full[kDfStages], empty[kDfStages];
+  __shared__ int wpos[kDfWarps];  // every position below wpos[w] that warp w owns is solved
+  __shared__ volatile int abort_flag;
+  const int p = blockIdx.x;
+  if (live && !live[p]) return;
+  const ProbDev& d = P[p];
+  const TriDesc T = UPPER ? d.U : d.L;
+  if (T.kind != TRI_DATAFLOW) return;  // solved by bsweep_tma
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int rmask = T.ring - 1;
+  double* rx = reinterpret_cast<double*>(smem + (size_t)kDfStages * T.stage);
+  int* rtag = reinterpret_cast<int*>(rx + 6 * (size_t)T.ring);
+  for (int t = tid; t < T.ring; t += kDfThreads) rtag[t] = -1;
+  if (tid < kDfWarps) wpos[tid] = 0;
+  if (tid == 0) {
+    for (int s = 0; s < kDfStages; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], kDfWarps);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    abort_flag = 0;
+  }
+  __syncthreads();
+  const unsigned long long wlim = g_wait_ns;
+  if (warp == kDfWarps) {  // producer
+    if (lane == 0) {
+      int issued = 0;
+      for (int c = 0; c < T.nch; c++) {
+        const int s = c % kDfStages;
+        if (c >= kDfStages) {  // the compute warps have released chunk c - kDfStages
+          const unsigned par = (unsigned)(((c / kDfStages) - 1) & 1);
+          const unsigned long long t0 = gtimer();
+          unsigned n = 0;
+          bool stop = false;
+          while (!mbar_try_wait(&empty[s], par))
+            if ((++n & 255u) == 0u && (abort_flag || gtimer() - t0 > wlim)) {
+              stop = true;
+              break;
+            }
+          if (stop) {
+            if (!abort_flag) {
+              abort_flag = 1;
+              atomicOr(&ctl->status, ST_TIMEOUT);
+            }
+            break;
+          }
+        }
+        const long long lo = T.off[c], hi = T.off[c + 1];
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect_tx(&full[s], (unsigned)(hi - lo));
+        bulk_g2s(smem + (size_t)s * T.stage, T.stream + lo, (unsigned)(hi - lo), &full[s]);
+        issued = c + 1;
+      }
+      // no copy may land after the CTA ends: the last stages' copies (all
+      // earlier ones were consumed before their stages were reused)
+      for (int q = max(0, issued - kDfStages); q < issued; q++)
+        mbar_wait(&full[q % kDfStages], (unsigned)((q / kDfStages) & 1), kWaitNs);
+    }
+    return;
+  }
+  const double* rb = rhs + 6 * (size_t)d.off;
+  double* ob = out + 6 * (size_t)d.off;
+  const int g = lane / 6, r = lane % 6;
+  // failure-injection knob for tests: warp 0 never publishes its rows
+  const bool publish = !(g_skip_meet && warp == 0);
+  int seen_min = 0;  // a lower bound of min(wpos)
+  bool ok = true;
+  auto fail = [&]() {
+    ok = false;
+    if (!abort_flag) {
+      abort_flag = 1;
+      atomicOr(&ctl->status, ST_TIMEOUT);
+    }
+  };
+  for (int c = 0; c < T.nch && ok; c++) {
+    const int s = c % kDfStages;
+    if (!mbar_wait(&full[s], (unsigned)((c / kDfStages) & 1), wlim)) fail();
+    if (__any_sync(0xffffffffu, !ok)) break;
+    const unsigned char* st = smem + (size_t)s * T.stage;
+    const int4 h = *reinterpret_cast<const int4*>(st);
+    const int nr = h.x, nb = h.y, p0 = h.z;
+    const int4* rec = reinterpret_cast<const int4*>(st + 16);
+    const int* dep = reinterpret_cast<const int*>(rec + nr);
+    const VT* val = reinterpret_cast<const VT*>(
+        st + ((16 + 16 * (size_t)nr + 4 * (size_t)nb + 15) & ~(size_t)15));
+    for (int k = warp; k < nr; k += kDfWarps) {
+      const int pos = p0 + k;
+      if (lane == 0) st_release_s32(&wpos[warp], pos);
+      const int4 row = rec[k];
+      const int i = row.x, b0 = row.y, cnt = row.z;
+      const double rv = lane < 6 ? rb[6 * (size_t)i + lane] : 0.0;
+      double acc = 0.0;
+      if (g < 4) {
+        for (int j = (UPPER ? 1 : 0) + g; j < cnt && ok; j += 4) {
+          const int q = dep[b0 + j];
+          const int* tg = &rtag[q & rmask];
+          if (ld_acquire_s32(tg) != q) {
+            const unsigned long long t0 = gtimer();
+            unsigned n = 0;
+            while (ld_acquire_s32(tg) != q)
+              if ((++n & 255u) == 0u && (abort_flag || gtimer() - t0 > wlim)) {
+                fail();
+                break;
+              }
+            if (!ok) break;
+          }
+          acc += dot6(val + (size_t)(b0 + j) * 36 + 6 * r, rx + 6 * (size_t)(q & rmask));
+        }
+      }
+      if (__any_sync(0xffffffffu, !ok)) {
+        ok = false;
+        break;
+      }
+      acc += __shfl_down_sync(0xffffffffu, acc, 12);
+      acc += __shfl_down_sync(0xffffffffu, acc, 6);
+      const double t = rv - acc;
+      double v = t;
+      if (UPPER) {
+        const VT* Di = val + (size_t)b0 * 36;
+        v = 0.0;
+#pragma unroll
+        for (int cc = 0; cc < 6; cc++) {
+          const double tc = __shfl_sync(0xffffffffu, t, cc);
+          if (lane < 6) v = fma((double)Di[6 * lane + cc], tc, v);
+        }
+      }
+      // flow control: the slot's previous position (pos - ring) is read
+      // only by rows at positions <= pos - ring + maxdist
+      const int slot = pos & rmask;
+      const int lim = pos - T.ring + T.maxdist;
+      if (lim >= seen_min) {
+        const unsigned long long t0 = gtimer();
+        while (true) {
+          int m = lane < kDfWarps ? ld_acquire_s32(&wpos[lane]) : 0x7fffffff;
+          m = __reduce_min_sync(0xffffffffu, m);
+          seen_min = m;
+          if (m > lim) break;
+          const int stop =
+              __shfl_sync(0xffffffffu, lane == 0 && (abort_flag || gtimer() - t0 > wlim), 0);
+          if (stop) {
+            if (lane == 0) fail();
+            ok = false;
+            break;
+          }
+        }
+        if (!ok) break;
+      }
+      if (lane < 6) {
+        rx[6 * slot + lane] = v;
+        ob[6 * (size_t)i + lane] = v;
+      }
+      __syncwarp();
+      if (lane == 0 && publish) st_release_s32(&rtag[slot], pos);
+    }
+    if (!ok) break;
+    __syncwarp();
+    if (lane == 0) {
+      mbar_arrive_local(&empty[s]);
+      st_release_s32(&wpos[warp], p0 + nr + warp);  // its first position in the next chunk
+    }
+  }
+  if (lane == 0) st_release_s32(&wpos[warp], 0x7fffffff);
+  if (ok && tid == 0 && bytes_ctr) atomicAdd(bytes_ctr, (unsigned long long)T.abytes);
 }
 
 // Factor values into a chunk stream: block slot q of the triangle takes
@@ -1028,6 +1242,7 @@ struct gf_precond {
   DevBuf<double> d_lu;
   struct Tri {
     int nch = 0, stage = 0, capb = 0, capr = 0, nsplit = 1;
+    int kind = TRI_LEVEL, ring = 0, maxdist = 0;
     size_t nslots = 0;
     long long abytes = 0;
     DevBuf<int64_t> off, vpos;
@@ -1239,19 +1454,151 @@ static cudaError_t build_tri(gf_precond* p, const std::vector<int32_t>& diag, bo
   up(t.stream.upload(bytes));
   return e;
 }
+// Stream of one triangle for the dataflow sweep (layout described at
+// TriDesc). Returns cudaSuccess with *used = false, building nothing, when
+// the triangle's ring and stages do not fit one CTA's shared memory.
+static cudaError_t build_df(gf_precond* p, const std::vector<int32_t>& diag, bool upper,
+                            bool* used) {
+  const Pattern& P = p->pat;
+  const int n = P.n;
+  const std::vector<int32_t>& lv = upper ? p->lvU : p->lvL;
+  const int nlev = upper ? p->nlevU : p->nlevL;
+  const size_t vs = p->prec == GF_PREC_FP32 ? 4 : 8;
+  *used = false;
+  // positions: rows by level, ties by row index
+  std::vector<int32_t> ptr(nlev + 1, 0), order(n), pos(n);
+  for (int i = 0; i < n; i++) ptr[lv[i] + 1]++;
+  for (int l = 0; l < nlev; l++) ptr[l + 1] += ptr[l];
+  {
+    std::vector<int32_t> f(ptr.begin(), ptr.end() - 1);
+    for (int i = 0; i < n; i++) order[f[lv[i]]++] = i;
+  }
+  for (int k = 0; k < n; k++) pos[order[k]] = k;
+  // a row's blocks: (position multiplied, factor block), U_ii^{-1} first in U
+  auto blocks = [&](int i, std::vector<std::pair<int32_t, int32_t>>& out) {
+    out.clear();
+    if (upper) {
+      for (int jp = diag[i] + 1; jp < P.rowp[i + 1]; jp++) out.emplace_back(pos[P.cols[jp]], jp);
+    } else {
+      for (int jp = P.rowp[i]; jp < diag[i]; jp++) out.emplace_back(pos[P.cols[jp]], jp);
+    }
+    std::sort(out.begin(), out.end());
+    if (upper) out.insert(out.begin(), std::make_pair(-1, diag[i]));
+  };
+  std::vector<std::pair<int32_t, int32_t>> bl;
+  int maxdist = 1, maxcnt = 0;
+  long long real = 0;
+  for (int i = 0; i < n; i++) {
+    blocks(i, bl);
+    maxcnt = std::max(maxcnt, (int)bl.size());
+    real += (long long)bl.size();
+    for (auto& b : bl)
+      if (b.first >= 0) maxdist = std::max(maxdist, pos[i] - b.first);
+  }
+  int ring = 64;
+  while (ring < 2 * (maxdist + 1)) ring *= 2;
+  const int capb = std::max(vs == 4 ? 256 : 128, maxcnt), capr = 64;
+  // chunks: consecutive positions, at most capb blocks and capr rows
+  std::vector<int32_t> ck{0};
+  {
+    int cb = 0, cr = 0;
+    for (int k = 0; k < n; k++) {
+      const int cnt = upper ? P.rowp[order[k] + 1] - diag[order[k]] : diag[order[k]] - P.rowp[order[k]];
+      if (cr > 0 && (cb + cnt > capb || cr == capr)) {
+        ck.push_back(k);
+        cb = cr = 0;
+      }
+      cb += cnt;
+      cr++;
+    }
+    ck.push_back(n);
+  }
+  const int nch = (int)ck.size() - 1;
+  std::vector<int64_t> off(nch + 1, 0);
+  auto head = [&](int c, int nb) {
+    return (16 + 16 * (int64_t)(ck[c + 1] - ck[c]) + 4 * (int64_t)nb + 15) & ~(int64_t)15;
+  };
+  std::vector<int32_t> nbc(nch, 0);
+  int stage = 0;
+  for (int c = 0; c < nch; c++) {
+    for (int k = ck[c]; k < ck[c + 1]; k++) {
+      const int i = order[k];
+      nbc[c] += upper ? P.rowp[i + 1] - diag[i] : diag[i] - P.rowp[i];
+    }
+    const int64_t bytes = head(c, nbc[c]) + 36 * (int64_t)vs * nbc[c];
+    off[c + 1] = off[c] + bytes;
+    stage = (int)std::max<int64_t>(stage, bytes);
+  }
+  if (df_smem_bytes(stage, ring) > kSweepSmemMax) return cudaSuccess;
+  std::vector<unsigned char> bytes(off[nch], 0);
+  const size_t nslots = (size_t)real;
+  std::vector<int32_t> map(nslots);
+  std::vector<int64_t> vpos(nslots);
+  size_t q = 0;
+  for (int c = 0; c < nch; c++) {
+    int32_t* w = reinterpret_cast<int32_t*>(bytes.data() + off[c]);
+    const int nr = ck[c + 1] - ck[c];
+    w[0] = nr;
+    w[1] = nbc[c];
+    w[2] = ck[c];
+    int32_t* rec = w + 4;
+    int32_t* dep = rec + 4 * nr;
+    const int64_t v0 = (off[c] + head(c, nbc[c])) / (int64_t)vs;
+    int b = 0;
+    for (int k = 0; k < nr; k++) {
+      const int i = order[ck[c] + k];
+      blocks(i, bl);
+      rec[4 * k + 0] = i;
+      rec[4 * k + 1] = b;
+      rec[4 * k + 2] = (int)bl.size();
+      for (auto& e : bl) {
+        dep[b] = e.first;
+        map[q] = e.second;
+        vpos[q] = v0 + 36 * (int64_t)b;
+        q++;
+        b++;
+      }
+    }
+  }
+  gf_precond::Tri& t = p->tri[upper ? 1 : 0];
+  t.kind = TRI_DATAFLOW;
+  t.nsplit = 1;
+  t.ring = ring;
+  t.maxdist = maxdist;
+  t.nch = nch;
+  t.stage = stage;
+  t.capb = capb;
+  t.capr = capr;
+  t.nslots = nslots;
+  t.abytes = real * (36 * (long long)vs + 4) + (long long)n * (4 + 48 + 48) + 4;
+  cudaError_t e = cudaSuccess;
+  auto up = [&](cudaError_t x) {
+    if (e == cudaSuccess) e = x;
+  };
+  up(t.off.upload(off));
+  up(t.vpos.upload(vpos));
+  up(t.map.upload(map));
+  up(t.stream.upload(bytes));
+  if (e == cudaSuccess) *used = true;
+  return e;
+}
 static TriDesc tri_desc(const gf_precond* p, int which) {
   const gf_precond::Tri& t = p->tri[which];
-  return TriDesc{t.nch, t.stage, t.capb, t.capr, t.off.p, t.stream.p, t.abytes, t.nsplit};
+  return TriDesc{t.nch,    t.stage,  t.capb, t.capr, t.off.p,   t.stream.p,
+                 t.abytes, t.nsplit, t.kind, t.ring, t.maxdist};
 }
 static size_t sweep_smem(const gf_precond* p, int which) {
   const gf_precond::Tri& t = p->tri[which];
-  return sweep_smem_bytes(t.stage, t.capb, t.capr);
+  return t.kind == TRI_DATAFLOW ? df_smem_bytes(t.stage, t.ring)
+                                : sweep_smem_bytes(t.stage, t.capb, t.capr);
 }
 }  // namespace gf
 
 struct gf_batch {
   int np = 0, nrows = 0, maxlevL = 0, maxlevU = 0;
-  size_t smemL = 0, smemU = 0;  // dynamic shared memory of the sweeps
+  size_t smemL = 0, smemU = 0;  // dynamic shared memory of the level-synchronous sweeps
+  size_t dfL = 0, dfU = 0;      // ... and of the dataflow sweeps
+  int nlevelL = 0, nlevelU = 0, ndfL = 0, ndfU = 0;  // problems solved by each kind
   int pprec = GF_PREC_FP64;      // factor precision shared by the batch's preconditioners
   size_t N = 0;  // doubles in batch space
   std::vector<gf_assembler*> asms;
@@ -1328,8 +1675,12 @@ static gf_status batch_build(gf_batch* B) {
   B->pprec = B->pcs[0]->prec;
   for (int k = 0; k < np; k++) {
     if (B->pcs[k]->prec != B->pprec) return GF_INVALID_ARG;  // one factor precision per batch
-    B->smemL = std::max(B->smemL, sweep_smem(B->pcs[k], 0));
-    B->smemU = std::max(B->smemU, sweep_smem(B->pcs[k], 1));
+    for (int w = 0; w < 2; w++) {
+      const bool df = B->pcs[k]->tri[w].kind == TRI_DATAFLOW;
+      size_t& sm = df ? (w ? B->dfU : B->dfL) : (w ? B->smemU : B->smemL);
+      sm = std::max(sm, sweep_smem(B->pcs[k], w));
+      (df ? (w ? B->ndfU : B->ndfL) : (w ? B->nlevelU : B->nlevelL))++;
+    }
     for (int i = 0; i < B->asms[k]->nnodes; i++) row_prob[B->offs[k] + i] = k;
     B->maxlevL = std::max(B->maxlevL, B->pcs[k]->nlevL);
     B->maxlevU = std::max(B->maxlevU, B->pcs[k]->nlevU);
@@ -1474,22 +1825,49 @@ static gf_status timing_begin(cudaStream_t st, unsigned long long** ctr, cudaEve
 // z = U^{-1} L^{-1} r for problems with live[p] (all when live is null).
 // The factor values are in the preconditioners' precision (one per batch),
 // independent of the precision of the Krylov loop that calls this.
+// One triangle of every problem of the batch: the dataflow kernel for the
+// problems whose triangle has a dataflow stream, the level-synchronous
+// kernel for the others (each kernel skips the other kind's problems).
+template <class VT, bool UPPER>
+static cudaError_t launch_tri(gf_batch* B, cudaStream_t st, const int* live, const double* rhs,
+                              double* out, unsigned long long* ctr) {
+  // the same caps for every batch: threads launching batches with different
+  // footprints concurrently must not lower them under each other
+  cudaError_t e = cudaSuccess;
+  if (UPPER ? B->ndfU : B->ndfL) {
+    e = cudaFuncSetAttribute(bsweep_df<VT, UPPER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kSweepSmemMax);
+    if (e != cudaSuccess) return e;
+    ::gf::count_launch();
+    bsweep_df<VT, UPPER><<<B->np, kDfThreads, UPPER ? B->dfU : B->dfL, st>>>(
+        B->d_desc.p, live, rhs, out, B->d_ctl.p, ctr);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  if (UPPER ? B->nlevelU : B->nlevelL) {
+    e = cudaFuncSetAttribute(bsweep_tma<VT, UPPER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kSweepSmemMax);
+    if (e != cudaSuccess) return e;
+    e = launch_sweep<VT, UPPER>(B->np, UPPER ? B->smemU : B->smemL, st, B->d_desc.p, live, rhs,
+                                out, B->d_ctl.p, ctr);
+  }
+  return e;
+}
+
+static bool sweeps_fit(const gf_batch* B) {
+  return B->smemL <= kSweepSmemMax && B->smemU <= kSweepSmemMax && B->dfL <= kSweepSmemMax &&
+         B->dfU <= kSweepSmemMax;
+}
+
+// y = L^{-1} r into tmp, z = U^{-1} y, for the problems with live[p].
 template <class VT>
-static gf_status bsweeps(gf_batch* B, const int* live, const double* r, double* z,
-                         cudaStream_t st) {
-  // the same cap for every batch: threads launching batches with different
-  // footprints concurrently must not lower it under each other
-  GF_CUDA(cudaFuncSetAttribute(bsweep_tma<VT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)kSweepSmemMax));
-  GF_CUDA(cudaFuncSetAttribute(bsweep_tma<VT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)kSweepSmemMax));
+static gf_status bsweeps(gf_batch* B, const int* live, const double* r, double* tmp, double* z,
+                         cudaStream_t st, bool timed) {
   unsigned long long* ctr = nullptr;
   cudaEvent_t e1 = nullptr;
-  if (timing_begin(st, &ctr, &e1) != GF_OK) return GF_CUDA_ERROR;
-  GF_CUDA((launch_sweep<VT, false>(B->np, B->smemL, st, B->d_desc.p, live, r, B->d_tmp.p,
-                                    B->d_ctl.p, ctr)));
-  GF_CUDA((launch_sweep<VT, true>(B->np, B->smemU, st, B->d_desc.p, live, B->d_tmp.p, z,
-                                   B->d_ctl.p, ctr)));
+  if (timed && timing_begin(st, &ctr, &e1) != GF_OK) return GF_CUDA_ERROR;
+  GF_CUDA((launch_tri<VT, false>(B, st, live, r, tmp, ctr)));
+  GF_CUDA((launch_tri<VT, true>(B, st, live, tmp, z, ctr)));
   GF_CHECK_LAUNCH();
   if (e1) GF_CUDA(cudaEventRecord(e1, st));
   return GF_OK;
@@ -1497,9 +1875,9 @@ static gf_status bsweeps(gf_batch* B, const int* live, const double* r, double* 
 template <class VT>
 static gf_status bprecond(gf_batch* B, const int* live, const double* r, double* z,
                           cudaStream_t st) {
-  if (B->smemL > kSweepSmemMax || B->smemU > kSweepSmemMax) return GF_INVALID_ARG;
-  return B->pprec == GF_PREC_FP32 ? bsweeps<float>(B, live, r, z, st)
-                                  : bsweeps<double>(B, live, r, z, st);
+  if (!sweeps_fit(B)) return GF_INVALID_ARG;
+  return B->pprec == GF_PREC_FP32 ? bsweeps<float>(B, live, r, B->d_tmp.p, z, st, true)
+                                  : bsweeps<double>(B, live, r, B->d_tmp.p, z, st, true);
 }
 
 template <class VT>
@@ -1885,7 +2263,13 @@ extern "C" {
 
 gf_status gf_precond_create(gf_assembler* a, int32_t fill_level, int32_t precision,
                             gf_precond** out) {
-  if (!a || !out || fill_level < 0 || (precision != GF_PREC_FP64 && precision != GF_PREC_FP32))
+  return gf_precond_create_ex(a, fill_level, precision, GF_SWEEP_AUTO, out);
+}
+
+gf_status gf_precond_create_ex(gf_assembler* a, int32_t fill_level, int32_t precision,
+                               int32_t sweep, gf_precond** out) {
+  if (!a || !out || fill_level < 0 || (precision != GF_PREC_FP64 && precision != GF_PREC_FP32) ||
+      sweep < GF_SWEEP_AUTO || sweep > GF_SWEEP_LEVEL)
     return GF_INVALID_ARG;
   gf_precond* p = new gf_precond();
   p->a = a;
@@ -1927,8 +2311,19 @@ gf_status gf_precond_create(gf_assembler* a, int32_t fill_level, int32_t precisi
   up(p->d_levLptr.upload(lptr));
   up(p->d_levLrows.upload(lrows));
   up(p->d_lu.alloc((size_t)36 * p->pat.nnz()));
-  if (e == cudaSuccess) e = build_tri(p, diag, false);
-  if (e == cudaSuccess) e = build_tri(p, diag, true);
+  for (int w = 0; w < 2 && e == cudaSuccess; w++) {
+    bool df = false;
+    if (sweep != GF_SWEEP_LEVEL) e = build_df(p, diag, w == 1, &df);
+    if (e == cudaSuccess && !df) {
+      if (sweep == GF_SWEEP_DATAFLOW) {
+        set_last_error_text("gf_precond_create_ex: the dataflow sweep's ring and stages of this "
+                            "factor do not fit one CTA's shared memory");
+        delete p;
+        return GF_INVALID_ARG;
+      }
+      e = build_tri(p, diag, w == 1);
+    }
+  }
   auto fits = [&](int w) {
     return sweep_smem(p, w) <= kSweepSmemMax;
   };
@@ -1970,6 +2365,19 @@ gf_status gf_precond_layout(const gf_precond* p, int32_t* nsplit_L, int32_t* nsp
   if (fac_split) *fac_split = fac_split_of(p);
   if (chunks_L) *chunks_L = p->tri[0].nch;
   if (chunks_U) *chunks_U = p->tri[1].nch;
+  return GF_OK;
+}
+
+gf_status gf_precond_sweeps(const gf_precond* p, int32_t* kind_L, int32_t* kind_U,
+                            int32_t* ring_L, int32_t* ring_U) {
+  if (!p) return GF_INVALID_ARG;
+  auto kind = [](const gf_precond::Tri& t) {
+    return t.kind == TRI_DATAFLOW ? GF_SWEEP_DATAFLOW : GF_SWEEP_LEVEL;
+  };
+  if (kind_L) *kind_L = kind(p->tri[0]);
+  if (kind_U) *kind_U = kind(p->tri[1]);
+  if (ring_L) *ring_L = p->tri[0].ring;
+  if (ring_U) *ring_U = p->tri[1].ring;
   return GF_OK;
 }
 
@@ -2055,35 +2463,17 @@ gf_status gf_precond_apply_noalloc(gf_precond* p, const double* d_r, double* d_z
     }
     y = g_noalloc_ptr[dev];
   }
-  if (B->smemL > kSweepSmemMax || B->smemU > kSweepSmemMax) {
+  if (!sweeps_fit(B)) {
     set_last_error_text("gf_precond_apply_noalloc: the sweeps need more shared memory than a "
                         "CTA has");
     return GF_INVALID_ARG;
   }
-  cudaStream_t st = as_stream(stream);
-  // the same two sweep kernels as gf_precond_apply; y in the fixed array and
-  // z written straight into d_z (a batch of one starts at offset 0)
-  if (p->prec == GF_PREC_FP32) {
-    GF_CUDA(cudaFuncSetAttribute(bsweep_tma<float, false>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSweepSmemMax));
-    GF_CUDA(cudaFuncSetAttribute(bsweep_tma<float, true>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSweepSmemMax));
-    GF_CUDA((launch_sweep<float, false>(1, B->smemL, st, B->d_desc.p, nullptr, d_r, y,
-                                        B->d_ctl.p, nullptr)));
-    GF_CUDA((launch_sweep<float, true>(1, B->smemU, st, B->d_desc.p, nullptr, y, d_z, B->d_ctl.p,
-                                       nullptr)));
-  } else {
-    GF_CUDA(cudaFuncSetAttribute(bsweep_tma<double, false>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSweepSmemMax));
-    GF_CUDA(cudaFuncSetAttribute(bsweep_tma<double, true>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSweepSmemMax));
-    GF_CUDA((launch_sweep<double, false>(1, B->smemL, st, B->d_desc.p, nullptr, d_r, y,
-                                         B->d_ctl.p, nullptr)));
-    GF_CUDA((launch_sweep<double, true>(1, B->smemU, st, B->d_desc.p, nullptr, y, d_z, B->d_ctl.p,
-                                        nullptr)));
-  }
-  GF_CHECK_LAUNCH();
-  return GF_OK;
+  // the same two sweeps as gf_precond_apply; y in the fixed array and z
+  // written straight into d_z (a batch of one starts at offset 0)
+  const gf_status s = p->prec == GF_PREC_FP32
+                          ? bsweeps<float>(B, nullptr, d_r, y, d_z, as_stream(stream), false)
+                          : bsweeps<double>(B, nullptr, d_r, y, d_z, as_stream(stream), false);
+  return s;
 }
 
 gf_status gf_timing_enable(int32_t enable) {

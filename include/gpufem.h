@@ -178,7 +178,31 @@ enum { GF_PREC_FP64 = 0, GF_PREC_FP32 = 1 };
  * 290 for triangles whose levels are split over two CTAs. */
 gf_status gf_precond_create(gf_assembler* a, int32_t fill_level, int32_t precision,
                             gf_precond** out);
+/* Which triangular-sweep kernel solves a triangle of the factor (sweep
+ * argument of gf_precond_create_ex; no reference counterpart, cuSPARSE's
+ * bsrsv2 picks its own level scheme):
+ *  GF_SWEEP_DATAFLOW  one CTA per problem; each row waits only for the rows
+ *                     it multiplies (shared-memory result ring), no block
+ *                     barriers between levels;
+ *  GF_SWEEP_LEVEL     level-synchronous chunks, split over a 2-CTA cluster
+ *                     when levels are large;
+ *  GF_SWEEP_AUTO      the dataflow kernel where its result ring and stages
+ *                     fit one CTA's shared memory (a factor whose rows
+ *                     reach back more than ~1000 positions in level order
+ *                     does not fit), the level-synchronous one otherwise.
+ * Both give the same z up to the rounding of different summation orders. */
+enum { GF_SWEEP_AUTO = 0, GF_SWEEP_DATAFLOW = 1, GF_SWEEP_LEVEL = 2 };
+/* gf_precond_create with a choice of sweep kernel. GF_SWEEP_DATAFLOW fails
+ * with GF_INVALID_ARG (text in gf_last_error) where the dataflow kernel does
+ * not fit. */
+gf_status gf_precond_create_ex(gf_assembler* a, int32_t fill_level, int32_t precision,
+                               int32_t sweep, gf_precond** out);
 gf_status gf_precond_destroy(gf_precond* p);
+/* The sweep kernel of the L and U triangles (GF_SWEEP_DATAFLOW or
+ * GF_SWEEP_LEVEL) and, for dataflow triangles, the result ring's slots. Any
+ * pointer may be NULL. */
+gf_status gf_precond_sweeps(const gf_precond* p, int32_t* kind_L, int32_t* kind_U,
+                            int32_t* ring_L, int32_t* ring_U);
 /* copyValues + numeric factorization (precond.h:35-44; cusparseDbsrilu02 at
  * examples/iterative/gmres.cu:426-457). Level-scheduled on the device. */
 gf_status gf_precond_factor(gf_precond* p, gf_bsr* A, void* stream);

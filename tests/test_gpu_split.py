@@ -1,13 +1,18 @@
-"""GPU parity of the two-CTA cluster paths of the block ILU factorization and
-of the triangular sweeps, the paths the large batched problems run.
+"""GPU parity of the large-problem paths of the block ILU factorization and of
+the triangular sweeps, the paths the large batched problems run.
 
 Case: 256 x 128 clamped plate, t = 2 mm, natural node ordering, ILU(6):
 33,153 block rows and 1,281 levels per triangle, about 26 rows and 405 (L) /
-431 (U) blocks per level. So the factorization splits every level's rows
-over a 2-CTA cluster (more than 16 rows a level), both sweeps split every
-chunk over the two CTAs (more than 200 blocks a level), and with FP64
-factors each level spans two chunks (a split FP64 chunk holds at most 344
-blocks), so near and far x entries cross chunk and CTA boundaries.
+431 (U) blocks per level. The factorization splits every level's rows over a
+2-CTA cluster (more than 16 rows a level). The sweeps are checked in both
+kernels:
+- level-synchronous (forced): both sweeps split every chunk over the two
+  CTAs (more than 200 blocks a level), and with FP64 factors each level spans
+  two chunks (a split FP64 chunk holds at most 344 blocks), so near and far x
+  entries cross chunk and CTA boundaries;
+- dataflow (the default): every row waits only for the rows it multiplies,
+  through a 1024-slot result ring that its flow control recycles 32 times
+  per sweep.
 
 Checked, with FP64 and FP32 factor values:
 - the layout really is split (gf_precond_layout);
@@ -65,18 +70,25 @@ def _layout(P):
     return [x.value for x in v]
 
 
+@pytest.mark.parametrize("sweep", ["level", "dataflow"])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_split_factor_and_apply_match_oracle(big, precision):
+def test_split_factor_and_apply_match_oracle(big, precision, sweep):
     import torch
     from gpu_fem_b200.assembler import ILUk_Preconditioner
     from oracle import pyoracle as po
-    P = ILUk_Preconditioner(big["A"], fill_level=6, precision=precision)
+    P = ILUk_Preconditioner(big["A"], fill_level=6, precision=precision, sweep=sweep)
     nsL, nsU, fsplit, chL, chU = _layout(P)
     inf = P.info()
-    assert (nsL, nsU, fsplit) == (2, 2, 1), (nsL, nsU, fsplit)
-    if precision == "fp64":
-        # levels larger than one split chunk: more chunks than levels
-        assert chL > inf["levels_L"] and chU > inf["levels_U"], (chL, chU, inf)
+    assert fsplit == 1
+    kinds = P.sweeps()
+    assert kinds["L"] == kinds["U"] == sweep, kinds
+    if sweep == "level":
+        assert (nsL, nsU) == (2, 2), (nsL, nsU)
+        if precision == "fp64":
+            # levels larger than one split chunk: more chunks than levels
+            assert chL > inf["levels_L"] and chU > inf["levels_U"], (chL, chU, inf)
+    else:
+        assert kinds["ring_L"] == kinds["ring_U"] == 1024, kinds
     P.factor(big["K"])
     torch.cuda.synchronize()
     r2, c2, lu = P.get()
@@ -118,15 +130,16 @@ def _superlu(mesh, rowp, cols, vals, perm):
     return x.reshape(-1, 6)[perm].ravel()
 
 
+@pytest.mark.parametrize("sweep", ["level", "dataflow"])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_split_solve_matches_direct_solve(big, precision):
+def test_split_solve_matches_direct_solve(big, precision, sweep):
     import torch
     from gpu_fem_b200.assembler import ILUk_Preconditioner, SolveOptions, gmres_solve
     x_ref = big.get("x_ref")
     if x_ref is None:
         x_ref = big["x_ref"] = _superlu(big["mesh"], big["rowp"], big["cols"], big["vals"],
                                         big["A"].getBsrData()["perm"])
-    P = ILUk_Preconditioner(big["A"], fill_level=6, precision=precision)
+    P = ILUk_Preconditioner(big["A"], fill_level=6, precision=precision, sweep=sweep)
     P.factor(big["K"])
     b = torch.tensor(big["mesh"].loads, device="cuda")
     x = torch.zeros_like(b)
@@ -143,7 +156,7 @@ def test_split_problems_bitwise_alone_and_in_batch():
     meshes = [_plate(160, 80, 0.002, 1e3), _plate(192, 96, 0.003, 1.4e3)]
     bs = BatchSolver(meshes, ordering="natural", fill=6, tune=False)
     for P in bs.P32:
-        assert _layout(P)[:3] == [2, 2, 1]
+        assert _layout(P)[2] == 1 and P.sweeps()["L"] == "dataflow"
     stats = bs.step(True)
     assert all(s["rel_residual"] <= 1e-8 for s in stats), stats
     x_mix = [x.cpu().numpy().copy() for x in bs.xs]

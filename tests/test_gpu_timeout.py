@@ -1,14 +1,17 @@
 """Bounded device-side waits report GF_TIMEOUT and leave the context usable.
 
-The split factorization and the split sweeps meet the partner CTA of their
-cluster once per level / chunk on mbarriers with bounded waits. The test
-shortens the bound to 200 us and makes CTA rank 1 skip its meeting arrivals
-(gf_test_set_waits), so rank 0's wait runs out: the launch records a
-timeout, both CTAs still meet on the final cluster barrier, and the host
-reads GF_TIMEOUT from gf_precond_factor, gf_precond_status after an apply,
-and gf_gmres_solve. With the default bound restored, the same objects factor
-and solve correctly. No wait is removed, so nothing can hang, and nothing
-faults.
+The split factorization and the split (level-synchronous) sweeps meet the
+partner CTA of their cluster once per level / chunk on mbarriers with
+bounded waits; the dataflow sweep waits, bounded, for the result tags of the
+rows each row multiplies. The tests shorten the bound to 200 us and switch
+on gf_test_set_waits' failure injection: CTA rank 1 skips its meeting
+arrivals, and the dataflow sweep's warp 0 never publishes its rows, so the
+waits run out. The launches record a timeout, both CTAs of a cluster still
+meet on the final cluster barrier, every CTA lets its copies in flight land,
+and the host reads GF_TIMEOUT from gf_precond_factor, gf_precond_status after
+an apply, and gf_gmres_solve. With the default bound restored, the same
+objects factor and solve correctly. No wait is removed, so nothing can hang,
+and nothing faults.
 """
 import ctypes as C
 
@@ -26,7 +29,8 @@ def _status(P):
     return L.lib().gf_precond_status(P.h, C.c_void_p(torch.cuda.current_stream().cuda_stream))
 
 
-def test_timeout_reported_and_context_usable():
+@pytest.mark.parametrize("sweep", ["level", "dataflow"])
+def test_timeout_reported_and_context_usable(sweep):
     import torch
     from gpu_fem_b200 import _lib as L
     from gpu_fem_b200.assembler import (ElementAssembler, ILUk_Preconditioner, SolveOptions,
@@ -37,10 +41,12 @@ def test_timeout_reported_and_context_usable():
     A = ElementAssembler.from_mesh(mesh, ordering="natural")
     K = createBsrMat(A)
     A.add_jacobian(None, K, fuse_bcs=True)
-    P = ILUk_Preconditioner(A, fill_level=6, precision="fp64")
-    lay = [C.c_int32() for _ in range(5)]
-    L.check(lib.gf_precond_layout(P.h, *[C.byref(v) for v in lay]), "layout")
-    assert [v.value for v in lay[:3]] == [2, 2, 1]  # both sweeps and the factorization split
+    P = ILUk_Preconditioner(A, fill_level=6, precision="fp64", sweep=sweep)
+    lay = P.layout()
+    assert lay["fac_split"] == 1  # the factorization splits each level over two CTAs
+    assert P.sweeps()["L"] == sweep
+    if sweep == "level":  # both sweeps split every chunk over two CTAs
+        assert (lay["nsplit_L"], lay["nsplit_U"]) == (2, 2)
     P.factor(K)
     r = torch.tensor(np.random.default_rng(3).standard_normal(mesh.num_dof), device="cuda")
     z_ok = torch.zeros_like(r)

@@ -18,38 +18,41 @@ from gpu_fem_b200 import mesh as M
 pytestmark = pytest.mark.gpu
 
 
-def _factored(mesh, fill, precision, ordering="rcm"):
+def _factored(mesh, fill, precision, ordering="rcm", sweep="auto"):
     import torch
     from gpu_fem_b200.assembler import ElementAssembler, ILUk_Preconditioner, createBsrMat
     A = ElementAssembler.from_mesh(mesh, ordering=ordering)
     K = createBsrMat(A)
     A.add_jacobian(None, K, fuse_bcs=True)
-    P = ILUk_Preconditioner(A, fill_level=fill, precision=precision)
+    P = ILUk_Preconditioner(A, fill_level=fill, precision=precision, sweep=sweep)
     P.factor(K)
     torch.cuda.synchronize()
     return A, K, P
 
 
 def _case(name):
-    """24x12 jittered cantilever, RCM, ILU(2): one CTA per sweep. 160x80
-    clamped plate, natural ordering, ILU(6), 13,041 nodes (below the array's
-    43,690-node capacity): both sweeps split every chunk over a 2-CTA
-    cluster, so the intermediate vector in the fixed array is written by two
-    CTAs and read back through the result ring."""
-    if name == "single_cta":
-        return M.plate_config2(24, 12), 2, "rcm", 1
-    return (M.plate(160, 80, 1.0, 0.5, lambda x, y: 0.002 + 0 * x, "all_edges",
-                    lambda q: 1e3 + 0 * q[:, 0]), 6, "natural", 2)
+    """single_cta: 24x12 jittered cantilever, RCM, ILU(2), level-synchronous
+    sweeps on one CTA. split: 160x80 clamped plate, natural ordering, ILU(6),
+    13,041 nodes (below the array's 43,690-node capacity), level-synchronous
+    sweeps that split every chunk over a 2-CTA cluster, so the intermediate
+    vector in the fixed array is written by two CTAs. dataflow: the same
+    plate with the dataflow sweeps (the default kernel)."""
+    plate = M.plate(160, 80, 1.0, 0.5, lambda x, y: 0.002 + 0 * x, "all_edges",
+                    lambda q: 1e3 + 0 * q[:, 0])
+    return {"single_cta": (M.plate_config2(24, 12), 2, "rcm", "level", 1),
+            "split": (plate, 6, "natural", "level", 2),
+            "dataflow": (plate, 6, "natural", "dataflow", 1)}[name]
 
 
-@pytest.mark.parametrize("case", ["single_cta", "split"])
+@pytest.mark.parametrize("case", ["single_cta", "split", "dataflow"])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_noalloc_apply_matches_apply_twice(precision, case):
     import torch
     from gpu_fem_b200 import _lib as L
     lib = L.lib()
-    mesh, fill, ordering, nsplit = _case(case)
-    A, K, P = _factored(mesh, fill, precision, ordering)
+    mesh, fill, ordering, sweep, nsplit = _case(case)
+    A, K, P = _factored(mesh, fill, precision, ordering, sweep)
+    assert P.sweeps()["L"] == sweep
     ns = [C.c_int32(), C.c_int32()]
     assert lib.gf_precond_layout(P.h, C.byref(ns[0]), C.byref(ns[1]), None, None, None) == L.GF_OK
     assert (ns[0].value, ns[1].value) == (nsplit, nsplit)
