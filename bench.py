@@ -57,9 +57,10 @@ def _args():
     ap.add_argument("--assembly-case", action="store_true",
                     help="small profiling case: Jacobian assembly (fused BCs) of the 400x200 "
                          "jittered cantilever plate, 5 times (no JSON line)")
-    ap.add_argument("--sweep-case", action="store_true",
+    ap.add_argument("--sweep-case", choices=["dataflow", "level"], default=None,
                     help="small profiling case: the triangular sweeps of one 256x128 plate, "
-                         "natural ordering, ILU(6), FP32 factors, applied 5 times (no JSON line)")
+                         "natural ordering, ILU(6), FP32 factors, applied 5 times with the "
+                         "given sweep kernel (no JSON line)")
     return ap.parse_args()
 
 
@@ -107,11 +108,13 @@ def assembly_case():
     print("assembly case", A.get_nnzb())
 
 
-def sweep_case():
+def sweep_case(kind):
     """One preconditioner (256x128 clamped plate, t = 2 mm, natural ordering,
-    ILU(6), FP32 factors, ~150 MB of factor) applied 5 times: the small case
-    on which the sweep and factorization kernels are profiled (its levels
-    are large enough that both run on a two-CTA cluster)."""
+    ILU(6), FP32 factors, ~150 MB of factor) applied 5 times with the given
+    sweep kernel: the small case on which the sweep and factorization kernels
+    are profiled (its levels are large enough that the factorization and the
+    level-synchronous sweeps run on a two-CTA cluster). Prints the mean
+    event-timed apply (both sweeps)."""
     import torch
     from gpu_fem_b200 import mesh as M
     from gpu_fem_b200.assembler import ElementAssembler, ILUk_Preconditioner, createBsrMat
@@ -120,14 +123,19 @@ def sweep_case():
     A = ElementAssembler.from_mesh(m, ordering="natural")
     K = createBsrMat(A)
     A.add_jacobian(None, K, fuse_bcs=True)
-    P = ILUk_Preconditioner(A, fill_level=6, precision="fp32")
+    P = ILUk_Preconditioner(A, fill_level=6, precision="fp32", sweep=kind)
     P.factor(K)
     r = torch.randn(m.num_dof, dtype=torch.float64, device="cuda")
     z = torch.zeros_like(r)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    P.apply(r, z)
+    e0.record()
     for _ in range(5):
         P.apply(r, z)
+    e1.record()
     torch.cuda.synchronize()
-    print("sweep case", P.info(), float(z.abs().max()))
+    print("sweep case", kind, P.info(), P.sweeps(), f"{e0.elapsed_time(e1) / 5:.3f} ms per apply",
+          float(z.abs().max()))
 
 
 def _peaks():
@@ -405,7 +413,7 @@ def plain_fp64_run(bs):
 def main():
     args = _args()
     if args.sweep_case:
-        return sweep_case()
+        return sweep_case(args.sweep_case)
     if args.assembly_case:
         return assembly_case()
     if args.impl == "reference":

@@ -733,29 +733,37 @@ static cudaError_t launch_sweep(int np, size_t smem, cudaStream_t st, const Prob
 // block barriers: compute warp w solves the rows of every chunk whose
 // chunk-local index is w mod kDfWarps, and a row waits only for the rows it
 // multiplies. A solved row's x entries go to global memory (the result) and
-// to a shared-memory ring of the latest `ring` positions, tagged with the
-// position they hold; a consumer waits (bounded) until the tag of each slot
-// it reads shows the row it needs, with acquire / release ordering at CTA
-// scope. A row's blocks are ordered by the position they depend on, so the
-// lane groups multiply the long-solved rows while the latest ones finish.
-// Flow control keeps the ring safe: before overwriting a slot with position
-// p a warp waits until every warp has moved past p - ring + maxdist (so all
-// readers of the slot's previous position are done), using the positions
-// the warps publish in wpos[]. Every position below min(wpos) is solved, so
-// the warp holding that minimum can always proceed: nothing waits in a
-// cycle. The factor stream arrives through kDfStages shared-memory stages
-// filled by 1D bulk copies, which the last warp issues as the compute warps
-// release stages (a full / empty mbarrier pair per stage). All waits are
+// to a shared-memory ring of the latest `ring` positions; every ring slot
+// has an mbarrier whose phase k completes when position slot + k ring is
+// written, so a consumer waits (bounded, suspended in hardware rather than
+// spinning) on the phase of exactly the position it reads, with release /
+// acquire ordering at CTA scope. A row's blocks are ordered by the position
+// they depend on, so the lane groups multiply the long-solved rows while the
+// latest ones finish.
+// Flow control keeps the phases unambiguous: before overwriting a slot with
+// position p a warp waits until every warp has moved past p - ring + maxdist
+// (so all readers of the slot's previous position are done), using the
+// positions the warps publish in wpos[]. Every position below min(wpos) is
+// solved, so the warp holding that minimum can always proceed: nothing
+// waits in a cycle.
+// The factor stream arrives through kDfStages shared-memory stages filled by
+// 1D bulk copies, which a producer warp issues as the compute warps release
+// stages (full / empty mbarriers), and a gather warp copies each chunk's
+// right-hand sides into the chunk's stage with cp.async (completion counted
+// on a third mbarrier), so no row waits on a global load. All waits are
 // bounded; on a timeout the CTA records ST_TIMEOUT and ends after its copies
 // in flight have landed.
-constexpr int kDfThreads = 512;
-constexpr int kDfWarps = kDfThreads / 32 - 1;  // compute warps; the last warp issues copies
+constexpr int kDfThreads = 544;
+constexpr int kDfWarps = kDfThreads / 32 - 2;  // compute warps
+constexpr int kDfProducer = kDfWarps;          // issues the stage copies
+constexpr int kDfGather = kDfWarps + 1;        // gathers the right-hand sides
 constexpr int kDfStages = 4;
+constexpr int kDfRows = 64;                    // rows per chunk at most
 
-// dynamic shared memory of a dataflow sweep: the stages, the ring's x entries
-// (6 doubles) and tags (int)
+// dynamic shared memory of a dataflow sweep: the stages, their right-hand
+// sides, the ring's x entries (6 doubles) and mbarriers
 __host__ __device__ inline size_t df_smem_bytes(int stage, int ring) {
-  return kDfStages * (size_t)stage + (size_t)ring * (48 + 4);
+  return kDfStages * ((size_t)stage + 48 * (size_t)kDfRows) + (size_t)ring * (48 + 8);
 }
 __device__ __forceinline__ void mbar_arrive_local(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
@@ -768,6 +776,16 @@ __device__ __forceinline__ int ld_acquire_s32(const int* p) {
 __device__ __forceinline__ void st_release_s32(int* p, int v) {
   asm volatile("st.release.cta.shared.b32 [%0], %1;" ::"r"(smem_u32(p)), "r"(v) : "memory");
 }
+// arrive on `bar` once all of this thread's earlier cp.async copies have
+// landed (the arrival is not counted in advance)
+__device__ __forceinline__ void cp_async_arrive(uint64_t* bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void cp_async8_df(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src)
+               : "memory");
+}
 
 template <class VT, bool UPPER>
 __global__ void __launch_bounds__(kDfThreads) bsweep_df(const ProbDev* __restrict__ P,
@@ -776,7 +794,7 @@ __global__ void __launch_bounds__(kDfThreads) bsweep_df(const ProbDev* __restric
                                                        double* out, SweepCtl* ctl,
                                                        unsigned long long* bytes_ctr) {
   extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ uint64_t full[kDfStages], empty[kDfStages];
+  __shared__ uint64_t full[kDfStages], empty[kDfStages], rhsb[kDfStages];
   __shared__ int wpos[kDfWarps];  // every position below wpos[w] that warp w owns is solved
   __shared__ volatile int abort_flag;
   const int p = blockIdx.x;
@@ -785,43 +803,47 @@ __global__ void __launch_bounds__(kDfThreads) bsweep_df(const ProbDev* __restric
   const TriDesc T = UPPER ? d.U : d.L;
   if (T.kind != TRI_DATAFLOW) return;  // solved by bsweep_tma
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int rmask = T.ring - 1;
-  double* rx = reinterpret_cast<double*>(smem + (size_t)kDfStages * T.stage);
-  int* rtag = reinterpret_cast<int*>(rx + 6 * (size_t)T.ring);
-  for (int t = tid; t < T.ring; t += kDfThreads) rtag[t] = -1;
+  const int rmask = T.ring - 1, rlog = __ffs(T.ring) - 1;
+  // layout: stages | right-hand sides of the stages | ring x | ring mbarriers
+  double* srhs = reinterpret_cast<double*>(smem + (size_t)kDfStages * T.stage);
+  double* rx = srhs + (size_t)kDfStages * 6 * kDfRows;
+  uint64_t* rbar = reinterpret_cast<uint64_t*>(rx + 6 * (size_t)T.ring);
+  for (int t = tid; t < T.ring; t += kDfThreads) mbar_init(&rbar[t], 1);
   if (tid < kDfWarps) wpos[tid] = 0;
   if (tid == 0) {
     for (int s = 0; s < kDfStages; s++) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], kDfWarps);
+      mbar_init(&rhsb[s], 32);
     }
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     abort_flag = 0;
   }
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   __syncthreads();
   const unsigned long long wlim = g_wait_ns;
-  if (warp == kDfWarps) {  // producer
+  // bounded wait that also gives up once another warp has aborted
+  auto wait_bar = [&](uint64_t* bar, unsigned par) {
+    const unsigned long long t0 = gtimer();
+    unsigned n = 0;
+    while (!mbar_try_wait(bar, par))
+      if ((++n & 63u) == 0u && (abort_flag || gtimer() - t0 > wlim)) return false;
+    return true;
+  };
+  auto fail = [&]() {
+    if (!abort_flag) {
+      abort_flag = 1;
+      atomicOr(&ctl->status, ST_TIMEOUT);
+    }
+  };
+  if (warp == kDfProducer) {
     if (lane == 0) {
       int issued = 0;
       for (int c = 0; c < T.nch; c++) {
         const int s = c % kDfStages;
-        if (c >= kDfStages) {  // the compute warps have released chunk c - kDfStages
-          const unsigned par = (unsigned)(((c / kDfStages) - 1) & 1);
-          const unsigned long long t0 = gtimer();
-          unsigned n = 0;
-          bool stop = false;
-          while (!mbar_try_wait(&empty[s], par))
-            if ((++n & 255u) == 0u && (abort_flag || gtimer() - t0 > wlim)) {
-              stop = true;
-              break;
-            }
-          if (stop) {
-            if (!abort_flag) {
-              abort_flag = 1;
-              atomicOr(&ctl->status, ST_TIMEOUT);
-            }
-            break;
-          }
+        // the compute warps have released chunk c - kDfStages
+        if (c >= kDfStages && !wait_bar(&empty[s], (unsigned)(((c / kDfStages) - 1) & 1))) {
+          fail();
+          break;
         }
         const long long lo = T.off[c], hi = T.off[c + 1];
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -836,23 +858,40 @@ __global__ void __launch_bounds__(kDfThreads) bsweep_df(const ProbDev* __restric
     }
     return;
   }
-  const double* rb = rhs + 6 * (size_t)d.off;
+  if (warp == kDfGather) {
+    // the right-hand sides of each chunk's rows into the chunk's stage, as
+    // soon as the chunk's records have landed
+    const double* rb = rhs + 6 * (size_t)d.off;
+    for (int c = 0; c < T.nch; c++) {
+      const int s = c % kDfStages;
+      if (!wait_bar(&full[s], (unsigned)((c / kDfStages) & 1))) {
+        if (lane == 0) fail();
+        break;
+      }
+      const unsigned char* st = smem + (size_t)s * T.stage;
+      const int nr = reinterpret_cast<const int4*>(st)->x;
+      const int4* rec = reinterpret_cast<const int4*>(st + 16);
+      double* dst = srhs + (size_t)s * 6 * kDfRows;
+      for (int t = lane; t < 6 * nr; t += 32)
+        cp_async8_df(dst + t, rb + 6 * (size_t)rec[t / 6].x + t % 6);
+      cp_async_arrive(&rhsb[s]);
+    }
+    cp_async_wait_all();  // no copy may land after the CTA ends
+    return;
+  }
   double* ob = out + 6 * (size_t)d.off;
   const int g = lane / 6, r = lane % 6;
   // failure-injection knob for tests: warp 0 never publishes its rows
   const bool publish = !(g_skip_meet && warp == 0);
   int seen_min = 0;  // a lower bound of min(wpos)
   bool ok = true;
-  auto fail = [&]() {
-    ok = false;
-    if (!abort_flag) {
-      abort_flag = 1;
-      atomicOr(&ctl->status, ST_TIMEOUT);
-    }
-  };
   for (int c = 0; c < T.nch && ok; c++) {
     const int s = c % kDfStages;
-    if (!mbar_wait(&full[s], (unsigned)((c / kDfStages) & 1), wlim)) fail();
+    const unsigned par = (unsigned)((c / kDfStages) & 1);
+    if (!wait_bar(&full[s], par) || !wait_bar(&rhsb[s], par)) {
+      fail();
+      ok = false;
+    }
     if (__any_sync(0xffffffffu, !ok)) break;
     const unsigned char* st = smem + (size_t)s * T.stage;
     const int4 h = *reinterpret_cast<const int4*>(st);
@@ -861,26 +900,21 @@ __global__ void __launch_bounds__(kDfThreads) bsweep_df(const ProbDev* __restric
     const int* dep = reinterpret_cast<const int*>(rec + nr);
     const VT* val = reinterpret_cast<const VT*>(
         st + ((16 + 16 * (size_t)nr + 4 * (size_t)nb + 15) & ~(size_t)15));
+    const double* crhs = srhs + (size_t)s * 6 * kDfRows;
     for (int k = warp; k < nr; k += kDfWarps) {
       const int pos = p0 + k;
       if (lane == 0) st_release_s32(&wpos[warp], pos);
       const int4 row = rec[k];
       const int i = row.x, b0 = row.y, cnt = row.z;
-      const double rv = lane < 6 ? rb[6 * (size_t)i + lane] : 0.0;
+      const double rv = lane < 6 ? crhs[6 * k + lane] : 0.0;
       double acc = 0.0;
       if (g < 4) {
-        for (int j = (UPPER ? 1 : 0) + g; j < cnt && ok; j += 4) {
+        for (int j = (UPPER ? 1 : 0) + g; j < cnt; j += 4) {
           const int q = dep[b0 + j];
-          const int* tg = &rtag[q & rmask];
-          if (ld_acquire_s32(tg) != q) {
-            const unsigned long long t0 = gtimer();
-            unsigned n = 0;
-            while (ld_acquire_s32(tg) != q)
-              if ((++n & 255u) == 0u && (abort_flag || gtimer() - t0 > wlim)) {
-                fail();
-                break;
-              }
-            if (!ok) break;
+          if (!wait_bar(&rbar[q & rmask], (unsigned)((q >> rlog) & 1))) {
+            fail();
+            ok = false;
+            break;
           }
           acc += dot6(val + (size_t)(b0 + j) * 36 + 6 * r, rx + 6 * (size_t)(q & rmask));
         }
@@ -928,7 +962,7 @@ __global__ void __launch_bounds__(kDfThreads) bsweep_df(const ProbDev* __restric
         ob[6 * (size_t)i + lane] = v;
       }
       __syncwarp();
-      if (lane == 0 && publish) st_release_s32(&rtag[slot], pos);
+      if (lane == 0 && publish) mbar_arrive_local(&rbar[slot]);
     }
     if (!ok) break;
     __syncwarp();
@@ -1497,7 +1531,7 @@ static cudaError_t build_df(gf_precond* p, const std::vector<int32_t>& diag, boo
   }
   int ring = 64;
   while (ring < 2 * (maxdist + 1)) ring *= 2;
-  const int capb = std::max(vs == 4 ? 256 : 128, maxcnt), capr = 64;
+  const int capb = std::max(vs == 4 ? 224 : 112, maxcnt), capr = kDfRows;
   // chunks: consecutive positions, at most capb blocks and capr rows
   std::vector<int32_t> ck{0};
   {
