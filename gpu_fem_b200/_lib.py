@@ -18,6 +18,7 @@ GF_ORDER_NATURAL, GF_ORDER_RCM = 0, 1
 GF_ASSEMBLE_OVERWRITE, GF_ASSEMBLE_ADD, GF_ASSEMBLE_FUSE_BCS = 0, 1, 2
 GF_PREC_FP64, GF_PREC_FP32 = 0, 1
 GF_SWEEP_AUTO, GF_SWEEP_DATAFLOW, GF_SWEEP_LEVEL = 0, 1, 2
+GF_FILL_FULL = 0x7FFFFFFF
 
 
 class GpuFemError(RuntimeError):
@@ -107,6 +108,7 @@ SIGNATURES = {
     "gf_solve_opts_default": (None, [C.POINTER(gf_solve_opts)]),
     "gf_gmres_solve": (_I, [_P, _P, _P, _P, _P, C.POINTER(gf_solve_opts),
                             C.POINTER(gf_solve_stats), _P]),
+    "gf_direct_solve": (_I, [_P, _P, _P, _P, C.POINTER(gf_solve_stats), _P]),
     "gf_batch_create": (_I, [_I, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]),
     "gf_batch_destroy": (_I, [_P]),
     "gf_batch_assemble": (_I, [_P, _P]),

@@ -2645,6 +2645,40 @@ gf_status gf_gmres_solve(gf_assembler* a, gf_bsr* A, gf_precond* p, const double
   return gf_batch_solve(p->self, &d_b, &d_x, opts, stats, stream);
 }
 
+gf_status gf_direct_solve(gf_assembler* a, gf_bsr* A, const double* d_b, double* d_x,
+                          gf_solve_stats* stats, void* stream) {
+  if (!a || !A || !d_b || !d_x || A->a != a) return GF_INVALID_ARG;
+  gf_precond* p = nullptr;
+  gf_status s = gf_precond_create(a, GF_FILL_FULL, GF_PREC_FP64, &p);
+  if (s != GF_OK) return s;
+  s = gf_precond_factor(p, A, stream);
+  gf_solve_stats st{};
+  if (s == GF_OK) {
+    // x = (LU)^{-1} b is the first step of right-preconditioned GMRES from
+    // x = 0 with the complete factor; the further steps are FP64 iterative
+    // refinement, run until the residual stops falling (at most 4 steps)
+    const size_t n = (size_t)6 * a->nnodes;
+    cudaError_t e = cudaMemsetAsync(d_x, 0, sizeof(double) * n, as_stream(stream));
+    if (e != cudaSuccess) {
+      set_last_error("gf_direct_solve", e);
+      s = GF_CUDA_ERROR;
+    } else {
+      gf_solve_opts o;
+      gf_solve_opts_default(&o);
+      o.restart = 4;
+      o.max_iters = 4;
+      o.rtol = 1e-15;
+      o.side = 1;
+      s = gf_gmres_solve(a, A, p, d_b, d_x, &o, &st, stream);
+      if (s == GF_NOT_CONVERGED) s = GF_OK;  // a direct solve has no tolerance to miss
+      st.status = s;
+    }
+  }
+  if (stats) *stats = st;
+  gf_precond_destroy(p);
+  return s;
+}
+
 gf_status gf_bsr_spmv(gf_bsr* m, double alpha, const double* d_x, double beta, double* d_y,
                       void* stream) {
   if (!m || !d_x || !d_y) return GF_INVALID_ARG;

@@ -287,6 +287,26 @@ gf_status gf_gmres_solve(gf_assembler* a, gf_bsr* A, gf_precond* p, const double
                          double* d_x, const gf_solve_opts* opts, gf_solve_stats* stats,
                          void* stream);
 
+/* fill_level of gf_precond_create(_ex) that keeps every fill block: the
+ * complete block LU factor (no entry dropped), i.e. a direct solver. */
+#define GF_FILL_FULL 0x7fffffff
+/* CUSPARSE::direct_LU_solve_old (include/linalg/solvers/cusparse.h:16-192):
+ * the reference factors the matrix with bsrilu02 on a full-fill pattern (a
+ * complete block LU without pivoting) and runs two bsrsv2 triangular solves.
+ * Here: the symbolic full fill of A's pattern in the assembler's ordering,
+ * the block LU on the GPU (the ILU kernels with nothing dropped), the two
+ * triangular sweeps, then FP64 refinement through the same factor: four
+ * steps of right-preconditioned GMRES from x = 0, the first of which is
+ * x = (LU)^{-1} b (residuals with the FP64 A). d_b / d_x in
+ * natural order; stats->rel_residual is the final ||b - A x|| / ||b||.
+ * Returns GF_OK, GF_ZERO_PIVOT, GF_NAN or a CUDA / argument error; factor
+ * rows longer than the sweep kernels' shared-memory stages (large
+ * bandwidths) give GF_INVALID_ARG with the reason in gf_last_error. The
+ * factor is built and released inside the call; for repeated solves with
+ * one matrix, create a GF_FILL_FULL preconditioner and use gf_gmres_solve. */
+gf_status gf_direct_solve(gf_assembler* a, gf_bsr* A, const double* d_b, double* d_x,
+                          gf_solve_stats* stats, void* stream);
+
 /* ---- batched uneven solves ------------------------------------------- */
 /* A batch of independent problems (assembler + BSR matrix + preconditioner
  * each) solved together: SpMV, ILU factorization and both triangular sweeps
