@@ -52,7 +52,7 @@ def _args():
                     help="skip the plain (one problem at a time) FP64 GPU path")
     ap.add_argument("--tune", action="store_true",
                     help="re-run the fill autotuner instead of the committed table")
-    ap.add_argument("--serve-seconds", type=float, default=0.0,
+    ap.add_argument("--serve-seconds", type=float, default=8.0,
                     help="length of the Poisson request stream of the serving run (0 skips it)")
     ap.add_argument("--assembly-case", action="store_true",
                     help="small profiling case: Jacobian assembly (fused BCs) of the 400x200 "
@@ -64,30 +64,33 @@ def _args():
     return ap.parse_args()
 
 
-SERVE_RATE, SERVE_MAX_CLASS = 20.0, 6
+SERVE_RATE, SERVE_MAX_CLASS = 10.0, 4
 
 
 def serving_run(seconds):
-    """Continuous-batching server on a Poisson stream of plate and box
-    requests (rate 20/s, size classes 5e3..5.5e4 DOF, per-request thickness
-    field and load from the request seed), once with FP32 ILU factors
-    (mixed) and once with FP64 factors, each to a 1e-8 relative residual.
-    Size classes are built and their fill tuned before the stream starts."""
+    """Continuous-batching server on a Poisson stream of plate and stiffened-box
+    requests (rate 10/s, size classes 0..4 = 5e3..2.2e4 DOF, per-request
+    thickness field and load from the request seed), once with FP32 ILU
+    factors (mixed) and once with FP64 factors, each to a 1e-8 relative
+    residual. Size classes are built, their fill tuned and their slot groups
+    reserved before the stream starts."""
     from gpu_fem_b200 import serve
     out, fills, n = {}, None, 0
     for prec, name in (("fp32", "mixed"), ("fp64", "fp64")):
         reqs = serve.poisson_requests(rate=SERVE_RATE, duration=seconds, seed=99,
                                       max_class=SERVE_MAX_CLASS)
         n = len(reqs)
-        srv = serve.Server(budget_gb=40.0, streams=4, max_batch=16, precision=prec, fills=fills)
+        srv = serve.Server(budget_gb=40.0, streams=4, max_batch=8, precision=prec, fills=fills)
         srv.warm({(r.family, r.cls) for r in reqs})
         fills = dict(srv.fills)
         res = srv.run(reqs)
         out[name] = {k: res[k] for k in ("requests", "solved", "solves_per_s", "p50_ms", "p99_ms",
-                                          "wall_s")}
+                                          "wall_s", "reserved_gb")}
+        del srv
     out["stream"] = (f"Poisson {SERVE_RATE:g} req/s for {seconds:g} s, {n} requests, plates and "
-                     f"stiffened boxes, size classes 0..{SERVE_MAX_CLASS} (5e3..5.5e4 DOF); "
-                     f"latency = completion - arrival")
+                     f"stiffened boxes, size classes 0..{SERVE_MAX_CLASS} (5e3..2.2e4 DOF); "
+                     f"latency = completion - arrival; slot groups of 8/4/2/1 per class reserved "
+                     f"before the stream")
     return out
 
 

@@ -316,11 +316,12 @@ __global__ void __launch_bounds__(kFacWarps * 32) bfactor_kernel(const ProbDev* 
         double u[kFacBatch][6];
 #pragma unroll
         for (int q = 0; q < kFacBatch; q++) {
+          // the values do not wait for the column index (both in flight)
           const int jp = u0 + 5 * q + b;
-          jc[q] = (lane < 30 && jp < u1) ? cols[jp] : -1;
-          if (jc[q] >= 0)
+          const bool in = lane < 30 && jp < u1;
+          jc[q] = in ? cols[jp] : -1;
 #pragma unroll
-            for (int m = 0; m < 6; m++) u[q][m] = LU[36 * (size_t)jp + 6 * m + c];
+          for (int m = 0; m < 6; m++) u[q][m] = in ? LU[36 * (size_t)jp + 6 * m + c] : 0.0;
         }
         const double* Ukk = LU + 36 * (size_t)diag[k];
         double* Aik = LU + 36 * (size_t)kp;
@@ -348,10 +349,10 @@ __global__ void __launch_bounds__(kFacWarps * 32) bfactor_kernel(const ProbDev* 
 #pragma unroll
             for (int q = 0; q < kFacBatch; q++) {
               const int jp = jb + 5 * q + b;
-              jc[q] = (lane < 30 && jp < u1) ? cols[jp] : -1;
-              if (jc[q] >= 0)
+              const bool in = lane < 30 && jp < u1;
+              jc[q] = in ? cols[jp] : -1;
 #pragma unroll
-                for (int m = 0; m < 6; m++) u[q][m] = LU[36 * (size_t)jp + 6 * m + c];
+              for (int m = 0; m < 6; m++) u[q][m] = in ? LU[36 * (size_t)jp + 6 * m + c] : 0.0;
             }
           }
           int tp[kFacBatch];

@@ -3,13 +3,17 @@
 Requests (a plate or a stiffened box, a size class, a per-request thickness
 field and load, all generated from the request seed) arrive as a Poisson
 stream. The server keeps, per size class, one device-resident assembler
-(mesh, node ordering, BSR pattern, coloured scatter schedule) and a pool of
-slots (BSR matrix, ILU(k) symbolic + factors, load / displacement vectors).
-A request is admitted when its slot memory fits the HBM budget; admitted
-requests are batched and solved with the batched engine (gf_batch_*) on a
-pool of CUDA streams served by worker threads, so requests that arrive
-while others are on the device start as soon as a slot and a stream free
-up, and their work overlaps on the device. Latency = completion - arrival.
+(mesh, node ordering, BSR pattern, coloured scatter schedule) and slot
+groups reserved before the stream starts: groups of 8, 4, 2 and 1 slots
+(BSR matrix, ILU(k) symbolic + factor streams, load / displacement /
+thickness vectors) with a persistent batch handle and solver workspace
+each, as many as the class's share of the HBM budget holds (measured).
+Nothing is allocated while requests stream in. A request is admitted when a
+reserved group of its class is free; the dispatcher fills the best-fitting
+free group with the class's queued requests and a worker thread runs it on
+its own CUDA stream with the batched engine (gf_batch_*), so requests that
+arrive while others are on the device start as soon as a group frees up,
+and batches overlap on the device. Latency = completion - arrival.
 
 Each request is solved with its own per-problem GMRES state and reductions,
 so its result does not depend on what else is in the batch (tested).
@@ -22,14 +26,14 @@ import math
 import queue
 import threading
 import time
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 
 import numpy as np
 import torch
 
 from . import _lib as L
 from . import mesh as M
-from .assembler import BsrMat, ElementAssembler, ILUk_Preconditioner, _stream
+from .assembler import BsrMat, ILUk_Preconditioner, _stream
 from .batch import Batch, BatchSolver, choose_ordering, solve_opts
 
 import ctypes as C
@@ -98,20 +102,55 @@ def poisson_requests(rate, duration, seed=99, nclasses=16, families=("plate", "b
     return reqs
 
 
+class Group:
+    """A fixed set of slots of one size class with a persistent batch handle:
+    a dispatch fills up to len(slots) requests into it; slots it leaves empty
+    get a zero load and drop out of the solve at its first residual check."""
+
+    def __init__(self, cls, size):
+        self.cls = cls
+        self.slots = [cls.make_slot() for _ in range(size)]
+        self.batch = Batch([cls.asm] * size, [s["K"] for s in self.slots],
+                           [s["P"] for s in self.slots])
+        n = size
+        self.thick_ptrs = (C.c_void_p * n)(*[s["thick"].data_ptr() for s in self.slots])
+
+    def run(self, reqs, server):
+        """Assemble, factor and solve the group with `reqs` in its first slots."""
+        cls = self.cls
+        for k, slot in enumerate(self.slots):
+            if k < len(reqs):
+                thick, loads = cls.request_data(reqs[k].seed)
+                slot["thick"].copy_(torch.from_numpy(thick), non_blocking=False)
+                slot["b"].copy_(torch.from_numpy(loads), non_blocking=False)
+            else:
+                slot["b"].zero_()
+            slot["x"].zero_()
+        L.check(L.lib().gf_batch_assemble_ex(self.batch.h, self.thick_ptrs, _stream()),
+                "assemble")
+        self.batch.factor()
+        st, stats = self.batch.solve([s["b"] for s in self.slots], [s["x"] for s in self.slots],
+                                     solve_opts(server.rtol, False, server.restart,
+                                                server.max_iters))
+        torch.cuda.current_stream().synchronize()
+        return stats[:len(reqs)]
+
+
 class SizeClass:
+    """Device-resident mesh, ordering, pattern and scatter schedule of one size
+    class, with slot groups reserved at warm-up (nothing is allocated while
+    requests stream in)."""
+
     def __init__(self, family, k, dof, fill=None, rtol=1e-8, precision="fp32"):
         self.family, self.k = family, k
         self.mesh = class_mesh(family, dof)
         self.ordering, self.asm = choose_ordering(self.mesh)
         self.fill = fill if fill is not None else tune_class_fill(self.mesh, self.ordering, rtol)
         self.precision = precision
-        self.free = []
+        self.groups = []       # reserved
+        self.free = []         # groups not running
         self.lock = threading.Lock()
-        nn, ne = self.mesh.num_nodes, self.mesh.num_elements
-        # per-slot footprint estimate: FP64+FP32 matrix, FP64+FP32 factors, vectors
-        nnzb = self.asm.get_nnzb()
-        self.slot_bytes = int(nnzb * 36 * 12 * (1 + 1.5 * (self.fill > 0)) * 2 + 6 * nn * 8 * 8 +
-                              ne * 8)
+        self.reserved_bytes = 0
 
     def make_slot(self):
         K = BsrMat(self.asm)
@@ -119,7 +158,42 @@ class SizeClass:
         n = self.mesh.num_dof
         return {"K": K, "P": P, "b": torch.zeros(n, dtype=torch.float64, device="cuda"),
                 "x": torch.zeros(n, dtype=torch.float64, device="cuda"),
-                "thick": torch.zeros(self.mesh.num_elements, dtype=torch.float64, device="cuda")}
+                "thick": torch.tensor(self.mesh.thick, dtype=torch.float64, device="cuda")}
+
+    def reserve(self, sizes, budget_bytes, server):
+        """Builds slot groups of the given sizes (largest first) while the
+        device memory they take (measured) stays within budget_bytes; each
+        group is run once with zero loads so its solver workspace exists
+        before the stream starts. Returns the bytes reserved."""
+        for size in sorted(sizes, reverse=True):
+            torch.cuda.synchronize()
+            before = torch.cuda.mem_get_info()[0]
+            g = Group(self, size)
+            g.run([], server)
+            used = before - torch.cuda.mem_get_info()[0]
+            if self.groups and self.reserved_bytes + used > budget_bytes:
+                del g  # over this class's share: released again
+                continue
+            self.reserved_bytes += used
+            self.groups.append(g)
+            self.free.append(g)
+        return self.reserved_bytes
+
+    def take_group(self, pending):
+        """The free group that best fits `pending` requests: the smallest one
+        that holds them all, else the largest free one; None if none is free."""
+        with self.lock:
+            if not self.free:
+                return None
+            fits = [g for g in self.free if len(g.slots) >= pending]
+            g = (min(fits, key=lambda x: len(x.slots)) if fits
+                 else max(self.free, key=lambda x: len(x.slots)))
+            self.free.remove(g)
+            return g
+
+    def give_back(self, g):
+        with self.lock:
+            self.free.append(g)
 
     def request_data(self, seed):
         """Thickness field and load vector of a request (from its seed)."""
@@ -135,11 +209,18 @@ class SizeClass:
 
 
 class Server:
-    def __init__(self, budget_gb=120.0, streams=4, max_batch=64, classes=None, restart=100,
+    """Continuous batching over reserved slot groups. Admission: a request
+    waits in its class's queue until a reserved group of the class is free;
+    the dispatcher then moves up to the group's size of queued requests into
+    it and hands it to a worker thread, which runs it on its own CUDA stream,
+    so batches of different classes (and several of one class) overlap on
+    the device while new requests keep arriving."""
+
+    GROUP_SIZES = (8, 4, 2, 1)
+
+    def __init__(self, budget_gb=120.0, streams=4, max_batch=8, classes=None, restart=100,
                  rtol=1e-8, fills=None, max_iters=3000, precision="fp32"):
         self.budget = budget_gb * 1e9
-        self.used = 0.0
-        self.mem_lock = threading.Lock()
         self.max_batch = max_batch
         self.restart, self.rtol, self.max_iters = restart, rtol, max_iters
         self.precision = precision  # ILU factor values: "fp32" (mixed) or "fp64"
@@ -149,10 +230,10 @@ class Server:
         self.completed = []
         self.done_lock = threading.Lock()
         self.errors = []
-        self.class_spec = classes or []
         self.fills = fills or {}
         self.keep_results = False
         self.results = {}
+        self.reserved_bytes = 0
 
     def get_class(self, family, k):
         key = (family, k)
@@ -163,11 +244,16 @@ class Server:
             self.fills[key] = self.classes[key].fill
         return self.classes[key]
 
-    def warm(self, keys, slots=1):
+    def warm(self, keys):
+        """Builds the size classes and reserves their slot groups (sizes up to
+        max_batch), the HBM budget shared equally by the classes."""
+        keys = sorted(keys)
+        share = self.budget / max(len(keys), 1)
+        sizes = [s for s in self.GROUP_SIZES if s <= self.max_batch]
         for fam, k in keys:
             c = self.get_class(fam, k)
-            for _ in range(slots):
-                c.free.append(c.make_slot())
+            if not c.groups:
+                self.reserved_bytes += c.reserve(sizes, share, self)
         torch.cuda.synchronize()
 
     def _worker(self, stream):
@@ -175,65 +261,47 @@ class Server:
             item = self.work.get()
             if item is None:
                 break
-            batch = item
+            group, reqs = item
             try:
                 with torch.cuda.stream(stream):
-                    self._run_batch(batch)
+                    stats = group.run(reqs, self)
+                now = time.perf_counter()
+                for req, s in zip(reqs, stats):
+                    req.done = now
+                    req.rel = s["rel_residual"]
+                    req.iters = s["iterations"]
+                    req.status = s["status"]
+                if self.keep_results:
+                    for req, slot in zip(reqs, group.slots):
+                        self.results[req.rid] = slot["x"].cpu().numpy().copy()
             except Exception as e:  # keep serving; record the failure
                 self.errors.append(repr(e))
-                for req, cls, slot in batch:
+                for req in reqs:
                     req.status = -2
                     req.done = time.perf_counter()
             finally:
-                for req, cls, slot in batch:
-                    with cls.lock:
-                        cls.free.append(slot)
-                    with self.mem_lock:
-                        self.used -= cls.slot_bytes
+                group.cls.give_back(group)
                 with self.done_lock:
-                    self.completed += [r for r, _, _ in batch]
-
-    def _run_batch(self, batch):
-        asms = [cls.asm for _, cls, _ in batch]
-        mats = [slot["K"] for _, _, slot in batch]
-        pcs = [slot["P"] for _, _, slot in batch]
-        for req, cls, slot in batch:
-            thick, loads = cls.request_data(req.seed)
-            slot["thick"].copy_(torch.from_numpy(thick), non_blocking=False)
-            slot["b"].copy_(torch.from_numpy(loads), non_blocking=False)
-            slot["x"].zero_()
-        bt = Batch(asms, mats, pcs)
-        n = len(batch)
-        T = (C.c_void_p * n)(*[slot["thick"].data_ptr() for _, _, slot in batch])
-        L.check(L.lib().gf_batch_assemble_ex(bt.h, T, _stream()), "assemble")
-        bt.factor()
-        st, stats = bt.solve([s["b"] for _, _, s in batch], [s["x"] for _, _, s in batch],
-                             solve_opts(self.rtol, False, self.restart, self.max_iters))
-        torch.cuda.current_stream().synchronize()
-        now = time.perf_counter()
-        for (req, _, slot), s in zip(batch, stats):
-            req.done = now
-            req.rel = s["rel_residual"]
-            req.iters = s["iterations"]
-            req.status = s["status"]
-            if self.keep_results:
-                self.results[req.rid] = slot["x"].cpu().numpy().copy()
+                    self.completed += reqs
 
     def solve_alone(self, req):
-        """Solve one request by itself (batch of one) and return x."""
+        """Solve one request by itself (a group of one built for it) and return x."""
         cls = self.get_class(req.family, req.cls)
-        slot = cls.make_slot()
-        self._run_batch([(req, cls, slot)])
+        g = Group(cls, 1)
+        g.run([req], self)
         torch.cuda.synchronize()
-        return slot["x"].cpu().numpy().copy()
+        return g.slots[0]["x"].cpu().numpy().copy()
 
     def run(self, requests, time_scale=1.0):
         """Serve a request stream in real time; returns per-request records."""
+        missing = {(r.family, r.cls) for r in requests} - set(self.classes)
+        if missing:
+            raise ValueError(f"size classes not warmed: {sorted(missing)}")
         threads = [threading.Thread(target=self._worker, args=(s,), daemon=True)
                    for s in self.streams]
         for t in threads:
             t.start()
-        pending = []
+        queues = {key: [] for key in self.classes}
         i = 0
         t_start = time.perf_counter()
         nreq = len(requests)
@@ -241,41 +309,23 @@ class Server:
             now = time.perf_counter() - t_start
             while i < nreq and requests[i].arrival * time_scale <= now:
                 requests[i].t0 = t_start + requests[i].arrival * time_scale
-                pending.append(requests[i])
+                queues[(requests[i].family, requests[i].cls)].append(requests[i])
                 i += 1
-            # admit FIFO while slots and memory allow; one batch per size class
-            # (requests of a class cost alike, so none waits on a slower kind)
-            groups = {}
-            keep = []
-            for req in pending:
-                cls = self.get_class(req.family, req.cls)
-                batch = groups.setdefault((req.family, req.cls), [])
-                ok = len(batch) < self.max_batch
-                if ok:
-                    with self.mem_lock:
-                        ok = self.used + cls.slot_bytes <= self.budget
-                        if ok:
-                            self.used += cls.slot_bytes
-                if not ok:
-                    keep.append(req)
-                    continue
-                with cls.lock:
-                    slot = cls.free.pop() if cls.free else None
-                if slot is None:
-                    slot = cls.make_slot()
-                batch.append((req, cls, slot))
-            pending = keep
             dispatched = False
-            for batch in groups.values():
-                if batch:
-                    self.work.put(batch)
+            for key, q in queues.items():
+                while q:
+                    g = self.classes[key].take_group(len(q))
+                    if g is None:
+                        break
+                    take, q[:] = q[:len(g.slots)], q[len(g.slots):]
+                    self.work.put((g, take))
                     dispatched = True
             with self.done_lock:
                 ndone = len(self.completed)
-            if i >= nreq and not pending and ndone >= nreq:
+            if i >= nreq and ndone >= nreq:
                 break
             if not dispatched:
-                time.sleep(0.002)
+                time.sleep(0.001)
         for _ in threads:
             self.work.put(None)
         for t in threads:
@@ -286,4 +336,4 @@ class Server:
         return {"requests": nreq, "solved": len(ok), "wall_s": t_end - t_start,
                 "solves_per_s": len(ok) / (t_end - t_start),
                 "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                "errors": self.errors[:3]}
+                "reserved_gb": self.reserved_bytes / 1e9, "errors": self.errors[:3]}
