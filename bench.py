@@ -69,7 +69,7 @@ SERVE_RATE, SERVE_MAX_CLASS = 10.0, 4
 
 def serving_run(seconds):
     """Continuous-batching server on a Poisson stream of plate and stiffened-box
-    requests (rate 10/s, size classes 0..4 = 5e3..2.2e4 DOF, per-request
+    requests (rate 10/s, size classes 0..4 = 5e3..2.5e4 DOF, per-request
     thickness field and load from the request seed), once with FP32 ILU
     factors (mixed) and once with FP64 factors, each to a 1e-8 relative
     residual. Size classes are built, their fill tuned and their slot groups
@@ -88,7 +88,7 @@ def serving_run(seconds):
                                           "wall_s", "reserved_gb")}
         del srv
     out["stream"] = (f"Poisson {SERVE_RATE:g} req/s for {seconds:g} s, {n} requests, plates and "
-                     f"stiffened boxes, size classes 0..{SERVE_MAX_CLASS} (5e3..2.2e4 DOF); "
+                     f"stiffened boxes, size classes 0..{SERVE_MAX_CLASS} (5e3..2.5e4 DOF); "
                      f"latency = completion - arrival; slot groups of 8/4/2/1 per class reserved "
                      f"before the stream")
     return out

@@ -2348,7 +2348,7 @@ gf_status gf_precond_create_ex(gf_assembler* a, int32_t fill_level, int32_t prec
   up(p->d_lu.alloc((size_t)36 * p->pat.nnz()));
   for (int w = 0; w < 2 && e == cudaSuccess; w++) {
     bool df = false;
-    if (sweep != GF_SWEEP_LEVEL) e = build_df(p, diag, w == 1, &df);
+    if (sweep == GF_SWEEP_DATAFLOW) e = build_df(p, diag, w == 1, &df);
     if (e == cudaSuccess && !df) {
       if (sweep == GF_SWEEP_DATAFLOW) {
         set_last_error_text("gf_precond_create_ex: the dataflow sweep's ring and stages of this "

@@ -186,10 +186,11 @@ gf_status gf_precond_create(gf_assembler* a, int32_t fill_level, int32_t precisi
  *                     barriers between levels;
  *  GF_SWEEP_LEVEL     level-synchronous chunks, split over a 2-CTA cluster
  *                     when levels are large;
- *  GF_SWEEP_AUTO      the dataflow kernel where its result ring and stages
- *                     fit one CTA's shared memory (a factor whose rows
- *                     reach back more than ~1000 positions in level order
- *                     does not fit), the level-synchronous one otherwise.
+ *  GF_SWEEP_AUTO      the level-synchronous kernel (the faster of the two
+ *                     on the batched plate workload on B200).
+ * The dataflow kernel needs its result ring and stages to fit one CTA's
+ * shared memory: a factor whose rows reach back more than ~1000 positions
+ * in level order does not fit.
  * Both give the same z up to the rounding of different summation orders. */
 enum { GF_SWEEP_AUTO = 0, GF_SWEEP_DATAFLOW = 1, GF_SWEEP_LEVEL = 2 };
 /* gf_precond_create with a choice of sweep kernel. GF_SWEEP_DATAFLOW fails

@@ -6,13 +6,12 @@ Case: 256 x 128 clamped plate, t = 2 mm, natural node ordering, ILU(6):
 431 (U) blocks per level. The factorization splits every level's rows over a
 2-CTA cluster (more than 16 rows a level). The sweeps are checked in both
 kernels:
-- level-synchronous (forced): both sweeps split every chunk over the two
-  CTAs (more than 200 blocks a level), and with FP64 factors each level spans
-  two chunks (a split FP64 chunk holds at most 344 blocks), so near and far x
-  entries cross chunk and CTA boundaries;
-- dataflow (the default): every row waits only for the rows it multiplies,
-  through a 1024-slot result ring that its flow control recycles 32 times
-  per sweep.
+- level-synchronous (the default): both sweeps split every chunk over the
+  two CTAs (more than 200 blocks a level), and with FP64 factors each level
+  spans two chunks (a split FP64 chunk holds at most 344 blocks), so near and
+  far x entries cross chunk and CTA boundaries;
+- dataflow: every row waits only for the rows it multiplies, through a
+  1024-slot result ring that its flow control recycles 32 times per sweep.
 
 Checked, with FP64 and FP32 factor values:
 - the layout really is split (gf_precond_layout);
@@ -156,7 +155,8 @@ def test_split_problems_bitwise_alone_and_in_batch():
     meshes = [_plate(160, 80, 0.002, 1e3), _plate(192, 96, 0.003, 1.4e3)]
     bs = BatchSolver(meshes, ordering="natural", fill=6, tune=False)
     for P in bs.P32:
-        assert _layout(P)[2] == 1 and P.sweeps()["L"] == "dataflow"
+        lay = _layout(P)
+        assert lay[:3] == [2, 2, 1] and P.sweeps()["L"] == "level", lay
     stats = bs.step(True)
     assert all(s["rel_residual"] <= 1e-8 for s in stats), stats
     x_mix = [x.cpu().numpy().copy() for x in bs.xs]
