@@ -52,6 +52,8 @@ def _args():
                     help="skip the plain (one problem at a time) FP64 GPU path")
     ap.add_argument("--tune", action="store_true",
                     help="re-run the fill autotuner instead of the committed table")
+    ap.add_argument("--tune-log", default=None,
+                    help="with --tune: write the autotuner's trial log (JSON) to this file")
     ap.add_argument("--serve-seconds", type=float, default=8.0,
                     help="length of the Poisson request stream of the serving run (0 skips it)")
     ap.add_argument("--assembly-case", action="store_true",
@@ -568,6 +570,9 @@ def main():
     if fills is None or args.tune:
         line["tuned_table"] = {"fills": [int(k) for k in bs.fills],
                                "orders": "".join(o[0] for o in bs.orderings)}
+        if args.tune_log:
+            with open(args.tune_log, "w") as f:
+                json.dump([[str(x) for x in e] for e in (bs.tune_log or [])], f)
     if args.serve_seconds > 0:
         line["serving"] = serving_run(args.serve_seconds)
     if rank == 0 and not args.no_cpu_baseline and ws == 1:

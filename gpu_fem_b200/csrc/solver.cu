@@ -85,9 +85,24 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
       : "memory");
   return ok != 0;
 }
+// as mbar_try_wait, but the thread may be suspended (not spinning on issue
+// slots) until the phase completes or about hint_ns have passed
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t* bar, unsigned parity,
+                                                    unsigned hint_ns) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
+      : "memory");
+  return ok != 0;
+}
 // bounded wait; returns false if limit_ns passed first
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity,
                                           unsigned long long limit_ns) {
+  // the timer is read only once the first test fails (reading it is slow)
+  if (mbar_try_wait(bar, parity)) return true;
   const unsigned long long t0 = gtimer();
   unsigned n = 0;
   while (!mbar_try_wait(bar, parity)) {
@@ -127,7 +142,7 @@ __device__ __forceinline__ void mbar_arrive_remote(unsigned addr) {
 // bounded wait with acquire at cluster scope; false if limit_ns passed first
 __device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, unsigned parity,
                                                   unsigned long long limit_ns) {
-  const unsigned long long t0 = gtimer();
+  unsigned long long t0 = 0;
   unsigned n = 0;
   while (true) {
     unsigned ok;
@@ -138,6 +153,7 @@ __device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, unsigned parity
         : "r"(smem_u32(bar)), "r"(parity)
         : "memory");
     if (ok) return true;
+    if (n == 0) t0 = gtimer();  // read only once the first test fails (reading it is slow)
     if ((++n & 255u) == 0u && gtimer() - t0 > limit_ns) return false;
   }
 }
@@ -751,20 +767,26 @@ static cudaError_t launch_sweep(int np, size_t smem, cudaStream_t st, const Prob
 // 1D bulk copies, which a producer warp issues as the compute warps release
 // stages (full / empty mbarriers), and a gather warp copies each chunk's
 // right-hand sides into the chunk's stage with cp.async (completion counted
-// on a third mbarrier), so no row waits on a global load. All waits are
-// bounded; on a timeout the CTA records ST_TIMEOUT and ends after its copies
-// in flight have landed.
-constexpr int kDfThreads = 544;
-constexpr int kDfWarps = kDfThreads / 32 - 2;  // compute warps
+// on a third mbarrier), so no row waits on a global load. The compute warps
+// store nothing to global memory: a writer warp copies every solved row from
+// the ring to the result vector in position order (it waits on the same
+// slot barriers and takes part in the flow control), so the release
+// operations of the compute warps order shared-memory writes only and never
+// wait for global stores to complete. All waits are bounded; on a timeout
+// the CTA records ST_TIMEOUT and ends after its copies in flight have landed.
+constexpr int kDfThreads = 576;
+constexpr int kDfWarps = kDfThreads / 32 - 3;  // compute warps
 constexpr int kDfProducer = kDfWarps;          // issues the stage copies
 constexpr int kDfGather = kDfWarps + 1;        // gathers the right-hand sides
+constexpr int kDfWriter = kDfWarps + 2;        // writes results to global memory
 constexpr int kDfStages = 4;
 constexpr int kDfRows = 64;                    // rows per chunk at most
+constexpr int kDfWriteBatch = 64;              // positions the writer reports at once
 
 // dynamic shared memory of a dataflow sweep: the stages, their right-hand
-// sides, the ring's x entries (6 doubles) and mbarriers
+// sides, the ring's x entries (6 doubles), row indices and mbarriers
 __host__ __device__ inline size_t df_smem_bytes(int stage, int ring) {
-  return kDfStages * ((size_t)stage + 48 * (size_t)kDfRows) + (size_t)ring * (48 + 8);
+  return kDfStages * ((size_t)stage + 48 * (size_t)kDfRows) + (size_t)ring * (48 + 8 + 4);
 }
 __device__ __forceinline__ void mbar_arrive_local(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
@@ -796,7 +818,9 @@ __global__ void __launch_bounds__(kDfThreads) bsweep_df(const ProbDev* __restric
                                                        unsigned long long* bytes_ctr) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint64_t full[kDfStages], empty[kDfStages], rhsb[kDfStages];
-  __shared__ int wpos[kDfWarps];  // every position below wpos[w] that warp w owns is solved
+  // every position below wpos[w] that compute warp w owns is solved; every
+  // position below wpos[kDfWarps] has been written out by the writer warp
+  __shared__ int wpos[kDfWarps + 1];
   __shared__ volatile int abort_flag;
   const int p = blockIdx.x;
   if (live && !live[p]) return;
@@ -809,8 +833,9 @@ __global__ void __launch_bounds__(kDfThreads) bsweep_df(const ProbDev* __restric
   double* srhs = reinterpret_cast<double*>(smem + (size_t)kDfStages * T.stage);
   double* rx = srhs + (size_t)kDfStages * 6 * kDfRows;
   uint64_t* rbar = reinterpret_cast<uint64_t*>(rx + 6 * (size_t)T.ring);
+  int* ridx = reinterpret_cast<int*>(rbar + T.ring);  // row index of each slot's position
   for (int t = tid; t < T.ring; t += kDfThreads) mbar_init(&rbar[t], 1);
-  if (tid < kDfWarps) wpos[tid] = 0;
+  if (tid <= kDfWarps) wpos[tid] = 0;
   if (tid == 0) {
     for (int s = 0; s < kDfStages; s++) {
       mbar_init(&full[s], 1);
@@ -823,11 +848,15 @@ __global__ void __launch_bounds__(kDfThreads) bsweep_df(const ProbDev* __restric
   __syncthreads();
   const unsigned long long wlim = g_wait_ns;
   // bounded wait that also gives up once another warp has aborted
+  // Waiting warps sleep in the barrier test instead of spinning, so the warps
+  // that have work get the issue slots; the timer is read only once the
+  // first test fails.
   auto wait_bar = [&](uint64_t* bar, unsigned par) {
+    if (mbar_try_wait(bar, par)) return true;
     const unsigned long long t0 = gtimer();
     unsigned n = 0;
-    while (!mbar_try_wait(bar, par))
-      if ((++n & 63u) == 0u && (abort_flag || gtimer() - t0 > wlim)) return false;
+    while (!mbar_try_wait_sleep(bar, par, 2000u))
+      if ((++n & 15u) == 0u && (abort_flag || gtimer() - t0 > wlim)) return false;
     return true;
   };
   auto fail = [&]() {
@@ -881,6 +910,33 @@ __global__ void __launch_bounds__(kDfThreads) bsweep_df(const ProbDev* __restric
     return;
   }
   double* ob = out + 6 * (size_t)d.off;
+  const int n = d.n;
+  if (warp == kDfWriter) {
+    // lane group g5 (5 groups of 6 lanes) writes position q0 + g5
+    const int g5 = lane / 6, r6 = lane % 6;
+    bool okw = true;
+    for (int q0 = 0; q0 < n && okw; q0 += 5) {
+      const int q = q0 + g5;
+      if (lane < 30 && q < n) {
+        if (!wait_bar(&rbar[q & rmask], (unsigned)((q >> rlog) & 1))) {
+          fail();
+          okw = false;
+        } else {
+          const int slot = q & rmask;
+          ob[6 * (size_t)ridx[slot] + r6] = rx[6 * slot + r6];
+        }
+      }
+      if (__any_sync(0xffffffffu, !okw)) break;
+      const int next = q0 + 5;
+      // report progress every kDfWriteBatch positions; the release makes the
+      // slot reads above complete before any warp may overwrite the slots
+      if (next % kDfWriteBatch == 0 || next >= n) {
+        __syncwarp();
+        if (lane == 0) st_release_s32(&wpos[kDfWarps], next >= n ? 0x7fffffff : next);
+      }
+    }
+    return;
+  }
   const int g = lane / 6, r = lane % 6;
   // failure-injection knob for tests: warp 0 never publishes its rows
   const bool publish = !(g_skip_meet && warp == 0);
@@ -942,12 +998,13 @@ __global__ void __launch_bounds__(kDfThreads) bsweep_df(const ProbDev* __restric
       const int slot = pos & rmask;
       const int lim = pos - T.ring + T.maxdist;
       if (lim >= seen_min) {
-        const unsigned long long t0 = gtimer();
-        while (true) {
-          int m = lane < kDfWarps ? ld_acquire_s32(&wpos[lane]) : 0x7fffffff;
+        unsigned long long t0 = 0;
+        for (int it = 0;; it++) {
+          int m = lane <= kDfWarps ? ld_acquire_s32(&wpos[lane]) : 0x7fffffff;
           m = __reduce_min_sync(0xffffffffu, m);
           seen_min = m;
           if (m > lim) break;
+          if (it == 0) t0 = gtimer();
           const int stop =
               __shfl_sync(0xffffffffu, lane == 0 && (abort_flag || gtimer() - t0 > wlim), 0);
           if (stop) {
@@ -958,10 +1015,8 @@ __global__ void __launch_bounds__(kDfThreads) bsweep_df(const ProbDev* __restric
         }
         if (!ok) break;
       }
-      if (lane < 6) {
-        rx[6 * slot + lane] = v;
-        ob[6 * (size_t)i + lane] = v;
-      }
+      if (lane < 6) rx[6 * slot + lane] = v;
+      if (lane == 0) ridx[slot] = i;
       __syncwarp();
       if (lane == 0 && publish) mbar_arrive_local(&rbar[slot]);
     }
@@ -1530,8 +1585,12 @@ static cudaError_t build_df(gf_precond* p, const std::vector<int32_t>& diag, boo
     for (auto& b : bl)
       if (b.first >= 0) maxdist = std::max(maxdist, pos[i] - b.first);
   }
+  // the ring holds every position a row may still need (maxdist back) plus
+  // the lag of the progress the warps report (a chunk's rows for the compute
+  // warps, a report batch for the writer), so flow control never waits on a
+  // warp that is itself waiting
   int ring = 64;
-  while (ring < 2 * (maxdist + 1)) ring *= 2;
+  while (ring < 2 * (maxdist + 1) || ring < maxdist + 2 * kDfRows + kDfWriteBatch + 8) ring *= 2;
   const int capb = std::max(vs == 4 ? 224 : 112, maxcnt), capr = kDfRows;
   // chunks: consecutive positions, at most capb blocks and capr rows
   std::vector<int32_t> ck{0};
