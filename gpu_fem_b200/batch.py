@@ -33,7 +33,7 @@ import torch
 from . import _lib as L
 from .assembler import BsrMat, ElementAssembler, ILUk_Preconditioner, SolveOptions, _stream
 
-FILL_CANDIDATES = (0, 1, 2, 3, 4, 5, 6, 7, 8, 10, 12, 16, 24)
+FILL_CANDIDATES = (0, 1, 2, 3, 4, 5, 6, 7, 8, 10, 12, 16, 24)  # then GF_FILL_FULL (see _autotune)
 
 
 class Batch:
@@ -228,6 +228,39 @@ class BatchSolver:
         self.b32 = Batch(self.asms, self.mats, self.P32)
         torch.cuda.synchronize()
 
+    def _trial(self, k, todo, cap, best, cands, log):
+        """Factor and solve problems `todo` with fill k (FP32 factors inside
+        FP64 GMRES, at most `cap` steps); records the converging ones."""
+        try:
+            P = [ILUk_Preconditioner(self.asms[i], k, "fp32") for i in todo]
+        except L.GpuFemError:  # a factor row longer than the sweep's stage
+            log.append((k, "precond create failed"))
+            return False
+        bt = Batch([self.asms[i] for i in todo], [self.mats[i] for i in todo], P)
+        try:
+            bt.factor()
+        except L.GpuFemError:
+            log.append((k, "factor failed"))
+            return True
+        for i in todo:
+            self.xs[i].zero_()
+        st, stats = bt.solve([self.bs[i] for i in todo], [self.xs[i] for i in todo],
+                             solve_opts(self.rtol, False, restart=self.restart, max_iters=cap))
+        for j, i in enumerate(todo):
+            s = stats[j]
+            nrow = self.asms[i].get_num_nodes()
+            inf = dict(P[j].info(), nrow=nrow)
+            nlev = inf["levels_L"] + inf["levels_U"]
+            ok = s["status"] == L.GF_OK
+            log.append((i, k, s["iterations"], s["rel_residual"], nlev, ok))
+            if ok:
+                cands[i].append((k, s["iterations"], factor_cost_us(nrow, inf),
+                                 sweep_cost_us(inf)))
+                cost = step_cost_us(nrow, inf, s["iterations"])
+                if best[i] is None or cost < best[i][0]:
+                    best[i] = (cost, k, k)
+        return True
+
     def _autotune(self, cap=400):
         n = len(self.meshes)
         best = [None] * n
@@ -237,34 +270,8 @@ class BatchSolver:
             todo = [i for i in range(n) if best[i] is None or k <= best[i][2] + 4]
             if not todo:
                 break
-            try:
-                P = [ILUk_Preconditioner(self.asms[i], k, "fp32") for i in todo]
-            except L.GpuFemError:  # a factor row longer than the sweep's stage
-                log.append((k, "precond create failed"))
+            if not self._trial(k, todo, cap, best, cands, log):
                 break
-            bt = Batch([self.asms[i] for i in todo], [self.mats[i] for i in todo], P)
-            try:
-                bt.factor()
-            except L.GpuFemError:
-                log.append((k, "factor failed"))
-                continue
-            for i in todo:
-                self.xs[i].zero_()
-            st, stats = bt.solve([self.bs[i] for i in todo], [self.xs[i] for i in todo],
-                                 solve_opts(self.rtol, False, restart=self.restart, max_iters=cap))
-            for j, i in enumerate(todo):
-                s = stats[j]
-                nrow = self.asms[i].get_num_nodes()
-                inf = dict(P[j].info(), nrow=nrow)
-                nlev = inf["levels_L"] + inf["levels_U"]
-                ok = s["status"] == L.GF_OK
-                log.append((i, k, s["iterations"], s["rel_residual"], nlev, ok))
-                if ok:
-                    cands[i].append((k, s["iterations"], factor_cost_us(nrow, inf),
-                                     sweep_cost_us(inf)))
-                    cost = step_cost_us(nrow, inf, s["iterations"])
-                    if best[i] is None or cost < best[i][0]:
-                        best[i] = (cost, k, k)
             if all(b is not None for b in best) and k >= max(b[1] for b in best) + 4:
                 break
         missing = [self.meshes[i].name for i in range(n) if best[i] is None]
@@ -272,6 +279,17 @@ class BatchSolver:
             raise RuntimeError(f"no ILU fill level converged for {missing}")
         if self.objective == "problem":
             return [b[1] for b in best], log
+        # A batch runs as many GMRES steps as its slowest-converging problem
+        # needs: the problems that need many steps even at their best fill
+        # also get every higher fill and the complete factor (GF_FILL_FULL,
+        # a direct solve where its rows fit the sweep kernel) tried.
+        steps = [min(c[1] for c in cands[i]) for i in range(n)]
+        slow = [i for i in range(n) if steps[i] >= 0.6 * max(steps)]
+        for k in FILL_CANDIDATES + (L.GF_FILL_FULL,):
+            todo = [i for i in slow if all(c[0] != k for c in cands[i])
+                    and k > max(c[0] for c in cands[i])]
+            if todo:
+                self._trial(k, todo, cap, best, cands, log)
         fills, _ = choose_batch_fills(cands)
         return fills, log
 
