@@ -239,7 +239,7 @@ SWEEP_TRAFFIC = None
 # a B200. Both arms run every problem with these, so their configs match;
 # `--tune` re-runs the autotuner and prints the table it finds.
 FILLS = [6, 8, 5, 3, 4, 3, 4, 4, 4, 1, 4, 4, 3, 3, 7, 5, 5, 4, 3, 7, 3, 2, 4, 5, 3, 7, 3, 2, 3, 4,
-         4, 7, 3, 7, 3, 5, 5, 2, 2, 3, 16, 1, 3, 7, 3, 3, 5, 6, 5, 6, 2, 2, 12, 5, 3, 3, 3, 4, 6,
+         4, 7, 3, 7, 3, 5, 5, 2, 2, 3, 16, 7, 3, 7, 3, 3, 5, 6, 5, 6, 2, 2, 12, 5, 3, 3, 3, 4, 6,
          16, 2, 2, 3, 5]
 ORDERS = "n" * 64  # one character per problem: "n" natural, "r" RCM
 
