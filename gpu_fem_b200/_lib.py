@@ -55,6 +55,13 @@ class gf_solve_stats(C.Structure):
                 ("rel_residual", C.c_double), ("time_ms", C.c_double)]
 
 
+class gf_bdf_mesh(C.Structure):
+    _fields_ = [("num_nodes", C.c_int32), ("num_elements", C.c_int32), ("num_bcs", C.c_int32),
+                ("conn", C.POINTER(C.c_int32)), ("xpts", C.POINTER(C.c_double)),
+                ("bcs", C.POINTER(C.c_int32)), ("component", C.POINTER(C.c_int32)),
+                ("impl", C.c_void_p)]
+
+
 _P = C.c_void_p
 _I = C.c_int32
 _D = C.c_double
@@ -109,6 +116,8 @@ SIGNATURES = {
     "gf_gmres_solve": (_I, [_P, _P, _P, _P, _P, C.POINTER(gf_solve_opts),
                             C.POINTER(gf_solve_stats), _P]),
     "gf_direct_solve": (_I, [_P, _P, _P, _P, C.POINTER(gf_solve_stats), _P]),
+    "gf_bdf_read": (_I, [C.c_char_p, C.POINTER(C.POINTER(gf_bdf_mesh))]),
+    "gf_bdf_free": (_I, [C.POINTER(gf_bdf_mesh)]),
     "gf_batch_create": (_I, [_I, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]),
     "gf_batch_destroy": (_I, [_P]),
     "gf_batch_assemble": (_I, [_P, _P]),

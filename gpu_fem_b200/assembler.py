@@ -9,6 +9,7 @@ torch CUDA tensors; all compute goes through libgpufem.so.
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
 import torch
@@ -107,6 +108,19 @@ class ElementAssembler:
         self.bcs = bcs
 
     @classmethod
+    def createFromBDF(cls, path, E=70e9, nu=0.3, thick=0.005, ordering="natural", **kw):
+        """createFromBDF (include/assembler.h:92-115): the mesh of a NASTRAN
+        bulk-data file (read_bdf) with one material for every element, as
+        the reference's single `Data` argument; `thick` may also be a dict
+        from property id (PID) to thickness."""
+        m = read_bdf(path)
+        if isinstance(thick, dict):
+            t = np.array([thick[int(c)] for c in m["component"]], np.float64)
+        else:
+            t = thick
+        return cls(m["conn"], m["xpts"], m["bcs"], t, E, nu, ordering=ordering, **kw)
+
+    @classmethod
     def from_mesh(cls, mesh, ordering="natural", **kw):
         return cls(mesh.conn, mesh.xpts, mesh.bcs, mesh.thick, mesh.E, mesh.nu,
                    ordering=ordering, **kw)
@@ -192,6 +206,24 @@ class ElementAssembler:
 
 def _ip(a):
     return a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+def read_bdf(path):
+    """gf_bdf_read: conn (4 per element, tensor order), xpts, bcs (natural
+    DOF indices) and component (property id per element) of a NASTRAN
+    bulk-data file, as numpy arrays."""
+    mp = C.POINTER(L.gf_bdf_mesh)()
+    check(L.lib().gf_bdf_read(os.fsencode(path), C.byref(mp)), "gf_bdf_read")
+    try:
+        m = mp.contents
+        ne, nn, nb = m.num_elements, m.num_nodes, m.num_bcs
+        out = {"conn": np.ctypeslib.as_array(m.conn, (max(4 * ne, 1),))[:4 * ne].reshape(ne, 4).copy(),
+               "xpts": np.ctypeslib.as_array(m.xpts, (max(3 * nn, 1),))[:3 * nn].reshape(nn, 3).copy(),
+               "bcs": (np.ctypeslib.as_array(m.bcs, (nb,)).copy() if nb else np.zeros(0, np.int32)),
+               "component": np.ctypeslib.as_array(m.component, (max(ne, 1),))[:ne].copy()}
+    finally:
+        L.lib().gf_bdf_free(mp)
+    return out
 
 
 class BsrMat:

@@ -271,3 +271,58 @@ def batch_config4(n=64, seed=4321, E=70e9, nu=0.3):
                          lambda q, p=p: p + 0 * q[:, 0], E=E, nu=nu,
                          name=f"plate_{nx}x{ny}"))
     return out
+
+
+def write_bdf(mesh, path, fmt="small", node_ids=None, elem_ids=None, pid=1):
+    """Writes the mesh as a NASTRAN bulk-data file: GRID, CQUAD4 (nodes around
+    the element: tensor order n0 n1 n3 n2 becomes G1 G2 G3 G4 = n0 n1 n3 n2)
+    and one SPC entry per constrained node. fmt: "small" (8-column fields),
+    "large" (16-column fields, GRID* / CQUAD4* with '*' continuation lines) or
+    "free" (comma separated). node_ids / elem_ids: file ids (default 1..n)."""
+    nn, ne = mesh.num_nodes, mesh.num_elements
+    nid = np.arange(1, nn + 1) if node_ids is None else np.asarray(node_ids)
+    eid = np.arange(1, ne + 1) if elem_ids is None else np.asarray(elem_ids)
+    bc_nodes = {}
+    for d in np.asarray(mesh.bcs):
+        bc_nodes.setdefault(int(d) // 6, []).append(int(d) % 6 + 1)
+
+    def small(key, fields):
+        return key.ljust(8) + "".join(str(f)[:8].rjust(8) for f in fields)
+
+    def real8(x):
+        s = f"{x:.6g}"
+        if len(s) > 8:
+            s = f"{x:.2e}"
+        return s if ("." in s or "e" in s) else s + "."
+
+    lines = ["$ shell mesh", "BEGIN BULK"]
+    for k in range(nn):
+        x, y, z = mesh.xpts[k]
+        if fmt == "small":
+            lines.append(small("GRID", [nid[k], 0, real8(x), real8(y), real8(z)]))
+        elif fmt == "large":
+            f16 = [f"{float(v):.8e}" for v in (x, y, z)]  # at most 16 characters
+            lines.append("GRID*".ljust(8) + str(nid[k]).rjust(16) + "0".rjust(16) +
+                         f16[0].rjust(16) + f16[1].rjust(16))
+            lines.append("*".ljust(8) + f16[2].rjust(16))
+        else:
+            lines.append(f"GRID,{nid[k]},0,{float(x)!r},{float(y)!r},{float(z)!r}")
+    for e in range(ne):
+        c = mesh.conn[e]
+        g = [nid[c[0]], nid[c[1]], nid[c[3]], nid[c[2]]]
+        if fmt == "small":
+            lines.append(small("CQUAD4", [eid[e], pid] + g))
+        elif fmt == "large":
+            lines.append("CQUAD4*".ljust(8) + "".join(str(v).rjust(16) for v in [eid[e], pid] + g[:2]))
+            lines.append("*".ljust(8) + "".join(str(v).rjust(16) for v in g[2:]))
+        else:
+            lines.append("CQUAD4," + ",".join(str(v) for v in [eid[e], pid] + g))
+    for node, dofs in bc_nodes.items():
+        c = "".join(str(d) for d in sorted(dofs))
+        if fmt == "free":
+            lines.append(f"SPC,1,{nid[node]},{c},0.0")
+        else:
+            lines.append(small("SPC", [1, nid[node], c, "0."]))
+    lines.append("ENDDATA")
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")

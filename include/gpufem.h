@@ -150,6 +150,27 @@ gf_status gf_apply_bcs_vec(gf_assembler* a, double* d_vec, void* stream);
 /* apply_bcs(Mat) (include/assembler.h:137-154, bsr_mat.cuh:1-104). */
 gf_status gf_apply_bcs_mat(gf_assembler* a, gf_bsr* mat, void* stream);
 
+/* ---- BDF mesh input -------------------------------------------------- */
+/* A 4-node shell mesh read from a NASTRAN bulk-data file: the data
+ * TACSMeshLoader::scanBDFFile + getAssemblerCreatorData
+ * (include/mesh/TACSMeshLoader.h:188-225) hand to createFromBDF
+ * (include/assembler.h:92-115). GRID / GRID* (CP = CD = 0), CQUAD4 / CQUADR
+ * and SPC / SPC* entries in small-field, large-field or free-field format;
+ * nodes and elements are numbered by ascending file id; element nodes are in
+ * tensor order (G1 G2 G4 G3); bcs are natural DOF indices (6 node + dof).
+ * component[e] is the element's property id (PID). Other element types give
+ * GF_INVALID_ARG with the reason in gf_last_error. Host only. */
+typedef struct gf_bdf_mesh {
+  int32_t num_nodes, num_elements, num_bcs;
+  const int32_t* conn;       /* 4 per element */
+  const double* xpts;        /* 3 per node */
+  const int32_t* bcs;        /* ascending, unique */
+  const int32_t* component;  /* one per element */
+  void* impl;                /* owned by the library */
+} gf_bdf_mesh;
+gf_status gf_bdf_read(const char* path, gf_bdf_mesh** out);
+gf_status gf_bdf_free(gf_bdf_mesh* mesh);
+
 /* ---- BSR matrix ------------------------------------------------------ */
 /* createBsrMat (include/linalg/bsr_mat.h:354-357): values zeroed. */
 gf_status gf_bsr_create(gf_assembler* a, gf_bsr** out);

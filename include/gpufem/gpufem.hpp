@@ -16,7 +16,7 @@
 // handles own their memory (the reference's destructors are commented out,
 // vec.h:180-186); vectors at the boundary are in natural node order and the
 // solver ordering is applied inside; can_print flags are accepted and print
-// nothing; createFromBDF (BDF mesh input) is not provided.
+// nothing; TACSMeshLoader reads the 4-node shell subset of BDF input.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -173,6 +173,32 @@ struct BsrData {
 template <class Vec>
 class BsrMat;
 
+// TACSMeshLoader<T> (include/mesh/TACSMeshLoader.h:138-225), the part the
+// shell path uses: scanBDFFile reads GRID / CQUAD4 / SPC entries
+// (gf_bdf_read) and getAssemblerCreatorData hands them to createFromBDF.
+template <typename T>
+class TACSMeshLoader {
+ public:
+  TACSMeshLoader() = default;
+  TACSMeshLoader(const TACSMeshLoader&) = delete;
+  TACSMeshLoader& operator=(const TACSMeshLoader&) = delete;
+  ~TACSMeshLoader() {
+    if (m_) gf_bdf_free(m_);
+  }
+  int scanBDFFile(const char* file_name) {
+    if (m_) gf_bdf_free(m_);
+    m_ = nullptr;
+    check(gf_bdf_read(file_name, &m_), "scanBDFFile");
+    return 0;
+  }
+  int getNumNodes() const { return m_ ? m_->num_nodes : 0; }
+  int getNumElements() const { return m_ ? m_->num_elements : 0; }
+  const gf_bdf_mesh* data() const { return m_; }
+
+ private:
+  gf_bdf_mesh* m_ = nullptr;
+};
+
 // ElementAssembler<T, ElemGroup, Vec, Mat> (include/assembler.h:14-322).
 // Geo and vars connectivity must be identical for the shell element. The
 // node ordering of the solver (RCM by default here; the reference reorders
@@ -213,6 +239,20 @@ class ElementAssembler {
     h_.reset(a, [](gf_assembler* x) { gf_assembler_destroy(x); });
     xpts_ = xpts;
     conn_ = geo_conn;
+  }
+  // createFromBDF(mesh_loader, single_data) (include/assembler.h:92-115):
+  // every element gets the same material data
+  static ElementAssembler createFromBDF(TACSMeshLoader<T>& mesh_loader, Data single_data,
+                                        int ordering = GF_ORDER_RCM) {
+    const gf_bdf_mesh* m = mesh_loader.data();
+    if (!m) throw Error(GF_INVALID_ARG, "createFromBDF: no mesh scanned");
+    HostVec<int32_t> conn(4 * m->num_elements, m->conn);
+    HostVec<int> bcs(m->num_bcs, m->bcs);
+    HostVec<T> xpts(3 * m->num_nodes, m->xpts);
+    HostVec<Data> data(m->num_elements);
+    for (int e = 0; e < m->num_elements; e++) data[e] = single_data;
+    return ElementAssembler(m->num_nodes, m->num_nodes, m->num_elements, conn, conn, xpts, bcs,
+                            data, ordering);
   }
   // symbolic_factorization(fill, print) (include/assembler.h:76-81). The
   // reference widens the matrix pattern to the full LU fill here, for

@@ -3,7 +3,7 @@
 // examples/iterative/gmres.cu): template composition of the shell element,
 // ElementAssembler, createBsrMat, add_jacobian, apply_bcs, the direct LU
 // solve, ILUk_Preconditioner with GMRES, add_energy.
-// Usage: linear_static <mesh.bin> <output prefix>
+// Usage: linear_static <mesh.bin> <output prefix> [mesh.bdf]
 // mesh.bin (little-endian): int32 nn, ne, nbc; float64 E, nu; int32 conn[4 ne];
 // float64 xpts[3 nn]; int32 bcs[nbc]; float64 thick[ne]; float64 loads[6 nn].
 // Writes <prefix>.pattern (int32 nn, nnzb, rowPtr, colPtr, perm),
@@ -59,6 +59,12 @@ int main(int argc, char** argv) {
     HostVec<Data> physData(ne);
     for (int e = 0; e < ne; e++) physData[e] = Data(E, nu, th[e]);
     Assembler assembler(nn, nn, ne, geo_conn, geo_conn, xpts, bcs, physData);
+    if (argc > 3) {  // the same mesh from a BDF file: same counts
+      TACSMeshLoader<T> loader;
+      loader.scanBDFFile(argv[3]);
+      Assembler from_bdf = Assembler::createFromBDF(loader, physData[0]);
+      if (from_bdf.get_num_nodes() != nn || from_bdf.get_num_elements() != ne) return 6;
+    }
 
     bool print = false;
     assembler.symbolic_factorization(10.0, print);

@@ -53,8 +53,11 @@ def test_driver_runs_and_matches_oracle(oracle, driver, tmp_path):
     _write_mesh(mesh_path, m)
     prefix = str(tmp_path / "out")
     env = dict(os.environ)
-    r = subprocess.run([exe, mesh_path, prefix], capture_output=True, text=True, env=env,
-                       timeout=300)
+    args = [exe, mesh_path, prefix]
+    if driver.endswith(".cpp"):  # also TACSMeshLoader + createFromBDF
+        M.write_bdf(m, str(tmp_path / "mesh.bdf"), fmt="free")
+        args.append(str(tmp_path / "mesh.bdf"))
+    r = subprocess.run(args, capture_output=True, text=True, env=env, timeout=300)
     assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
     rowp, cols, perm, K, x_direct, x_gmres, info = _read(prefix, m)
     # the oracle in the same ordering
