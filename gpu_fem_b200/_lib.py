@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(_HERE, "libgpufem.so")
 
 GF_OK, GF_INVALID_ARG, GF_OOM, GF_ZERO_PIVOT, GF_NOT_CONVERGED, GF_NAN, GF_TIMEOUT, \
     GF_CUDA_ERROR, GF_NO_DEVICE, GF_OVER_BUDGET = range(10)
-GF_ORDER_NATURAL, GF_ORDER_RCM = 0, 1
+GF_ORDER_NATURAL, GF_ORDER_RCM, GF_ORDER_QORDER = 0, 1, 2
 GF_ASSEMBLE_OVERWRITE, GF_ASSEMBLE_ADD, GF_ASSEMBLE_FUSE_BCS = 0, 1, 2
 GF_PREC_FP64, GF_PREC_FP32 = 0, 1
 GF_SWEEP_AUTO, GF_SWEEP_DATAFLOW, GF_SWEEP_LEVEL = 0, 1, 2
@@ -40,7 +40,7 @@ class gf_mesh_desc(C.Structure):
                 ("conn", C.POINTER(C.c_int32)), ("xpts", C.POINTER(C.c_double)),
                 ("bcs", C.POINTER(C.c_int32)), ("num_bcs", C.c_int32),
                 ("data", C.POINTER(gf_shell_data)), ("ordering", C.c_int32),
-                ("rcm_root", C.c_int32)]
+                ("rcm_root", C.c_int32), ("qorder_p", C.c_double), ("qorder_seed", C.c_uint64)]
 
 
 class gf_solve_opts(C.Structure):
@@ -77,6 +77,7 @@ SIGNATURES = {
     "gf_launch_count": (C.c_longlong, []),
     "gf_assembler_create": (_I, [C.POINTER(gf_mesh_desc), C.POINTER(_P)]),
     "gf_assembler_destroy": (_I, [_P]),
+    "gf_order_nodes": (_I, [C.POINTER(gf_mesh_desc), _PI]),
     "gf_assembler_num_nodes": (_I, [_P]),
     "gf_assembler_num_elements": (_I, [_P]),
     "gf_assembler_num_vars": (_I, [_P]),

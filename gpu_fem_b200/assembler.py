@@ -76,7 +76,10 @@ class ElementAssembler:
     Built from a gpu_fem_b200.mesh.ShellMesh (or explicit arrays)."""
 
     def __init__(self, conn, xpts, bcs, thick, E=70e9, nu=0.3, ordering="natural",
-                 rcm_root=0, tOffset=0.0, ref_axis=None):
+                 rcm_root=0, tOffset=0.0, ref_axis=None, qorder_p=1.0, qorder_seed=0):
+        """ordering: "natural", "rcm" or "qorder" (deterministic q-ordering:
+        the RCM order shuffled within windows of bandwidth / qorder_p
+        positions, seeded with qorder_seed)."""
         conn = np.ascontiguousarray(conn, np.int32).reshape(-1, 4)
         xpts = np.ascontiguousarray(xpts, np.float64).reshape(-1, 3)
         bcs = np.ascontiguousarray(bcs, np.int32).ravel()
@@ -99,8 +102,11 @@ class ElementAssembler:
         desc.bcs = bcs.ctypes.data_as(C.POINTER(C.c_int32))
         desc.num_bcs = bcs.size
         desc.data = data
-        desc.ordering = {"natural": L.GF_ORDER_NATURAL, "rcm": L.GF_ORDER_RCM}[ordering]
+        desc.ordering = {"natural": L.GF_ORDER_NATURAL, "rcm": L.GF_ORDER_RCM,
+                         "qorder": L.GF_ORDER_QORDER}[ordering]
         desc.rcm_root = rcm_root
+        desc.qorder_p = qorder_p
+        desc.qorder_seed = qorder_seed
         h = C.c_void_p()
         torch.cuda.init()
         check(L.lib().gf_assembler_create(C.byref(desc), C.byref(h)), "gf_assembler_create")
@@ -206,6 +212,24 @@ class ElementAssembler:
 
 def _ip(a):
     return a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+def order_nodes(conn, num_nodes, ordering="rcm", rcm_root=0, qorder_p=1.0, qorder_seed=0):
+    """gf_order_nodes: the solver ordering perm[natural node] = row that an
+    assembler of this connectivity would use (host only)."""
+    conn = np.ascontiguousarray(conn, np.int32).reshape(-1, 4)
+    desc = L.gf_mesh_desc()
+    desc.num_nodes = num_nodes
+    desc.num_elements = conn.shape[0]
+    desc.conn = conn.ctypes.data_as(C.POINTER(C.c_int32))
+    desc.ordering = {"natural": L.GF_ORDER_NATURAL, "rcm": L.GF_ORDER_RCM,
+                     "qorder": L.GF_ORDER_QORDER}[ordering]
+    desc.rcm_root = rcm_root
+    desc.qorder_p = qorder_p
+    desc.qorder_seed = qorder_seed
+    perm = np.zeros(num_nodes, np.int32)
+    check(L.lib().gf_order_nodes(C.byref(desc), _ip(perm)), "gf_order_nodes")
+    return perm
 
 
 def read_bdf(path):

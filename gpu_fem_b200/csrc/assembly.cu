@@ -368,12 +368,7 @@ gf_status gf_assembler_create(const gf_mesh_desc* d, gf_assembler** out) {
   a->conn.assign(d->conn, d->conn + 4 * (size_t)ne);
   a->bcs.assign(d->bcs, d->bcs + d->num_bcs);
   a->pat0 = pattern_from_conn(ne, nn, d->conn);
-  if (d->ordering == GF_ORDER_RCM) {
-    rcm_order(a->pat0, d->rcm_root, 1, a->perm);
-  } else {
-    a->perm.resize(nn);
-    for (int i = 0; i < nn; i++) a->perm[i] = i;
-  }
+  order_nodes(a->pat0, d, a->perm);
   a->iperm.resize(nn);
   for (int i = 0; i < nn; i++) a->iperm[a->perm[i]] = i;
   a->pat = permute_pattern(a->pat0, a->perm);

@@ -78,6 +78,12 @@ Pattern pattern_from_conn(int nelem, int nnodes, const int32_t* conn);
 // TacsComputeRCMOrder (include/linalg/reordering_utils.h:189-291): rcm[old] = new.
 void rcm_order(const Pattern& p, int root, int iters, std::vector<int32_t>& rcm);
 Pattern permute_pattern(const Pattern& p, const std::vector<int32_t>& perm);
+int bandwidth(const Pattern& p);
+// deterministic q-ordering on top of an RCM order (examples/iterative/gmres.cu:159-215)
+void qorder(const Pattern& p, const std::vector<int32_t>& rcm, double pfac, uint64_t seed,
+            std::vector<int32_t>& out);
+// node ordering of a mesh description (GF_ORDER_*): perm[old] = new
+void order_nodes(const Pattern& p, const gf_mesh_desc* d, std::vector<int32_t>& perm);
 // get_elem_ind_map (include/linalg/bsr_utils.h:809-870); -1 if not found.
 void elem_ind_map(int nelem, const int32_t* conn, const Pattern& p,
                   const std::vector<int32_t>& perm, std::vector<int32_t>& map);

@@ -1,6 +1,8 @@
 // Host-side symbolic setup: block pattern, RCM, elemIndMap, ILU(k) pattern,
 // level sets and the coloured scatter schedule.
 #include <algorithm>
+#include <cstdlib>
+#include <random>
 #include <cstring>
 #include <numeric>
 
@@ -107,6 +109,42 @@ void elem_ind_map(int nelem, const int32_t* conn, const Pattern& p,
         map[16 * e + 4 * a + b] = (f != b1 && *f == c) ? (int32_t)(f - p.cols.data()) : -1;
       }
     }
+}
+
+// Bandwidth max |i - j| over the blocks of a pattern (getBandWidth,
+// include/linalg/bsr_utils.h:655-670).
+int bandwidth(const Pattern& p) {
+  int bw = 0;
+  for (int i = 0; i < p.n; i++)
+    for (int jp = p.rowp[i]; jp < p.rowp[i + 1]; jp++) bw = std::max(bw, std::abs(i - p.cols[jp]));
+  return bw;
+}
+
+// Deterministic q-ordering (examples/iterative/gmres.cu:159-215, which seeds
+// from std::random_device): the RCM order (perm[old] = new) is cut into
+// consecutive windows of floor(bandwidth / p) positions, bandwidth that of
+// the RCM-ordered pattern, and the positions inside each window are
+// permuted at random: a Fisher-Yates shuffle of the window's nodes (new
+// position -> node), from its last position down, swapping position i with
+// lo + (x mod (i - lo + 1)) for the next 64-bit output x of one MT19937-64
+// generator seeded with `seed` for the whole ordering.
+void qorder(const Pattern& p, const std::vector<int32_t>& rcm, double pfac, uint64_t seed,
+            std::vector<int32_t>& out) {
+  const int n = p.n;
+  const int bw = bandwidth(permute_pattern(p, rcm));
+  const int width = std::max(1, (int)((double)bw / (pfac > 0.0 ? pfac : 1.0)));
+  std::vector<int32_t> node(n);  // new position -> node
+  for (int i = 0; i < n; i++) node[rcm[i]] = i;
+  std::mt19937_64 g(seed);
+  for (int lo = 0; lo < n; lo += width) {
+    const int hi = std::min(n, lo + width);
+    for (int i = hi - 1; i > lo; i--) {
+      const int j = lo + (int)(g() % (uint64_t)(i - lo + 1));
+      std::swap(node[i], node[j]);
+    }
+  }
+  out.assign(n, 0);
+  for (int k = 0; k < n; k++) out[node[k]] = k;
 }
 
 Pattern iluk_pattern(const Pattern& a, int lev) {
@@ -298,3 +336,33 @@ int build_schedule(int nelem, int nnodes, const int32_t* conn, const std::vector
 }
 
 }  // namespace gf
+
+namespace gf {
+void order_nodes(const Pattern& p, const gf_mesh_desc* d, std::vector<int32_t>& perm) {
+  if (d->ordering == GF_ORDER_RCM || d->ordering == GF_ORDER_QORDER) {
+    rcm_order(p, d->rcm_root, 1, perm);
+    if (d->ordering == GF_ORDER_QORDER) {
+      std::vector<int32_t> q;
+      qorder(p, perm, d->qorder_p, d->qorder_seed, q);
+      perm.swap(q);
+    }
+  } else {
+    perm.resize(p.n);
+    for (int i = 0; i < p.n; i++) perm[i] = i;
+  }
+}
+}  // namespace gf
+
+extern "C" gf_status gf_order_nodes(const gf_mesh_desc* d, int32_t* perm) {
+  if (!d || !perm || d->num_nodes <= 0 || d->num_elements < 0 || !d->conn ||
+      d->ordering < GF_ORDER_NATURAL || d->ordering > GF_ORDER_QORDER)
+    return GF_INVALID_ARG;
+  for (int i = 0; i < 4 * d->num_elements; i++)
+    if (d->conn[i] < 0 || d->conn[i] >= d->num_nodes) return GF_INVALID_ARG;
+  if (d->rcm_root < 0 || d->rcm_root >= d->num_nodes) return GF_INVALID_ARG;
+  const gf::Pattern p = gf::pattern_from_conn(d->num_elements, d->num_nodes, d->conn);
+  std::vector<int32_t> v;
+  gf::order_nodes(p, d, v);
+  std::copy(v.begin(), v.end(), perm);
+  return GF_OK;
+}

@@ -64,9 +64,20 @@ typedef struct gf_mesh_desc {
   const gf_shell_data* data;   /* one per element */
   int32_t ordering;            /* GF_ORDER_* */
   int32_t rcm_root;            /* RCM root node (reference uses 0) */
+  double qorder_p;             /* GF_ORDER_QORDER: window = bandwidth / p (0: p = 1) */
+  uint64_t qorder_seed;        /* GF_ORDER_QORDER: seed of the window shuffles */
 } gf_mesh_desc;
 
-enum { GF_ORDER_NATURAL = 0, GF_ORDER_RCM = 1 };
+/* Node orderings of the solver: natural (the caller's numbering), RCM
+ * (TacsComputeRCMOrder, include/linalg/reordering_utils.h:189-291, root
+ * rcm_root), and q-ordering (examples/iterative/gmres.cu:159-215) made
+ * deterministic: the RCM order cut into windows of floor(bandwidth / p)
+ * positions (bandwidth of the RCM-ordered pattern, getBandWidth,
+ * include/linalg/bsr_utils.h:655-670), each window's positions permuted by a
+ * Fisher-Yates shuffle (from its last position down, position i swapped with
+ * lo + x mod (i - lo + 1)) drawing x from one MT19937-64 stream seeded with
+ * qorder_seed; the reference seeds from std::random_device. */
+enum { GF_ORDER_NATURAL = 0, GF_ORDER_RCM = 1, GF_ORDER_QORDER = 2 };
 
 enum { GF_ASSEMBLE_OVERWRITE = 0, GF_ASSEMBLE_ADD = 1, GF_ASSEMBLE_FUSE_BCS = 2 };
 
@@ -103,6 +114,10 @@ gf_status gf_timing_read(double* sweep_ms, long long* sweep_launches, double* sw
  * (include/linalg/bsr_utils.h:809-870), the coloured scatter schedule and
  * uploads the mesh to the current device. */
 gf_status gf_assembler_create(const gf_mesh_desc* desc, gf_assembler** out);
+/* The node ordering gf_assembler_create would use for this mesh
+ * (perm[natural node] = solver row, num_nodes entries). Host only: needs no
+ * GPU. */
+gf_status gf_order_nodes(const gf_mesh_desc* desc, int32_t* perm);
 gf_status gf_assembler_destroy(gf_assembler* a);
 /* get_num_nodes / get_num_elements / get_num_vars (include/assembler.h:117-118, :309-310) */
 int32_t gf_assembler_num_nodes(const gf_assembler* a);

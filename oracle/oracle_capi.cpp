@@ -25,6 +25,7 @@
 #include <cstdint>
 #include <cstring>
 #include <numeric>
+#include <random>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -151,6 +152,39 @@ int orc_rcm(int n, const int* rowp, const int* cols, int root, int n_iters, int*
     root = rcm_vars[0];
   }
   return rvars;
+}
+
+// Deterministic q-ordering on an RCM order rcm[old] = new (the intent of
+// examples/iterative/gmres.cu:159-215 with a fixed seed): bandwidth b =
+// max |i - j| of the RCM-ordered pattern (getBandWidth,
+// include/linalg/bsr_utils.h:655-670); windows of w = floor(b / pfac)
+// consecutive new positions; in each window, positions hi-1 down to lo+1
+// each swap their node with position lo + x mod (i - lo + 1), x the next
+// output of one std::mt19937_64(seed). out[old] = new.
+void orc_qorder(int n, const int* rowp, const int* cols, const int* rcm, double pfac,
+                unsigned long long seed, int* out) {
+  int bw = 0;
+  for (int i = 0; i < n; i++)
+    for (int jp = rowp[i]; jp < rowp[i + 1]; jp++) {
+      const int d = rcm[i] - rcm[cols[jp]];
+      bw = std::max(bw, d < 0 ? -d : d);
+    }
+  const double pp = pfac > 0.0 ? pfac : 1.0;
+  const int w = std::max(1, (int)((double)bw / pp));
+  std::vector<int> at(n);
+  for (int i = 0; i < n; i++) at[rcm[i]] = i;
+  std::mt19937_64 gen(seed);
+  for (int lo = 0; lo < n; lo += w) {
+    const int hi = std::min(n, lo + w);
+    for (int i = hi - 1; i > lo; i--) {
+      const unsigned long long x = gen();
+      const int j = lo + (int)(x % (unsigned long long)(i - lo + 1));
+      const int t = at[i];
+      at[i] = at[j];
+      at[j] = t;
+    }
+  }
+  for (int k = 0; k < n; k++) out[at[k]] = k;
 }
 
 // Permuted pattern P A P^T with ascending columns; perm[old] = new.

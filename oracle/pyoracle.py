@@ -125,6 +125,16 @@ def rcm(rowp, cols, root=0, iters=1):
     return out
 
 
+def qorder(rowp, cols, rcm_perm, pfac=1.0, seed=0):
+    """Deterministic q-ordering on top of an RCM order (perm[old] = new)."""
+    n = len(rowp) - 1
+    out = np.zeros(n, np.int32)
+    rcm_perm = np.ascontiguousarray(rcm_perm, np.int32)
+    lib().orc_qorder(n, _pi(rowp), _pi(cols), _pi(rcm_perm), C.c_double(pfac),
+                     C.c_ulonglong(seed), _pi(out))
+    return out
+
+
 def permute_pattern(rowp, cols, perm):
     n = len(rowp) - 1
     r2 = np.zeros(n + 1, np.int32)

@@ -203,3 +203,34 @@ def test_status_codes_zero_pivot_and_not_converged():
                                                         side=1), raise_on_fail=False)
     assert st == L.GF_NOT_CONVERGED
     assert stats["iterations"] <= 3 and stats["rel_residual"] > 1e-12
+
+
+def test_qordered_ilu_gmres_matches_dense_solve(oracle):
+    """The deterministic q-ordering (RCM shuffled within bandwidth-wide windows)
+    as the solver ordering: pattern and permutation as the oracle's, the
+    ILU(2)-GMRES displacement within 1e-8 of a dense FP64 solve."""
+    import torch
+    from gpu_fem_b200.assembler import (ElementAssembler, ILUk_Preconditioner, SolveOptions,
+                                        createBsrMat, gmres_solve)
+    m = M.plate(16, 16, 1.0, 1.0, lambda x, y: 0.006 + 0 * x, "all_edges",
+                lambda q: 1e3 + 0 * q[:, 0])
+    A = ElementAssembler.from_mesh(m, ordering="qorder", qorder_p=1.0, qorder_seed=42)
+    K = createBsrMat(A)
+    A.add_jacobian(None, K, fuse_bcs=True)
+    bd = A.getBsrData()
+    rowp0, cols0 = oracle.bsr_pattern(m.conn, m.num_nodes)
+    perm = oracle.qorder(rowp0, cols0, oracle.rcm(rowp0, cols0, 0, 1), 1.0, 42)
+    np.testing.assert_array_equal(bd["perm"], perm)
+    rowp, cols, vals, _, _ = oracle.assemble_jacobian(m, perm=perm)
+    oracle.apply_bcs_mat(rowp, cols, vals, perm, m.bcs)
+    b = np.zeros(m.num_dof)
+    b.reshape(-1, 6)[perm] = m.loads.reshape(-1, 6)
+    xd = oracle.dense_solve(oracle.bsr_to_dense(rowp, cols, vals), b).reshape(-1, 6)[perm].ravel()
+    P = ILUk_Preconditioner(A, fill_level=2)
+    P.factor(K)
+    bt = torch.tensor(m.loads, device="cuda")
+    x = torch.zeros_like(bt)
+    st, stats = gmres_solve(A, K, P, bt, x, SolveOptions(restart=200, max_iters=4000, rtol=1e-10))
+    assert stats["rel_residual"] <= 1e-10, stats
+    err = np.linalg.norm(x.cpu().numpy() - xd) / np.linalg.norm(xd)
+    assert err <= 1e-8, err
