@@ -82,13 +82,18 @@ def serving_run(seconds):
         reqs = serve.poisson_requests(rate=SERVE_RATE, duration=seconds, seed=99,
                                       max_class=SERVE_MAX_CLASS)
         n = len(reqs)
-        srv = serve.Server(budget_gb=40.0, streams=4, max_batch=8, precision=prec, fills=fills)
-        srv.warm({(r.family, r.cls) for r in reqs})
-        fills = dict(srv.fills)
-        res = srv.run(reqs)
-        out[name] = {k: res[k] for k in ("requests", "solved", "solves_per_s", "p50_ms", "p99_ms",
-                                          "wall_s", "reserved_gb")}
-        del srv
+        try:
+            srv = serve.Server(budget_gb=40.0, streams=4, max_batch=8, precision=prec,
+                               fills=fills)
+            srv.warm({(r.family, r.cls) for r in reqs})
+            fills = dict(srv.fills)
+            res = srv.run(reqs)
+            out[name] = {k: res[k] for k in ("requests", "solved", "solves_per_s", "p50_ms",
+                                              "p99_ms", "wall_s", "reserved_gb")}
+            out[name]["fills"] = {f"{f}{k}": int(v) for (f, k), v in sorted(srv.fills.items())}
+            del srv
+        except Exception as e:  # report the failure in the line, keep the rest
+            out[name] = {"error": repr(e)[:300]}
     out["stream"] = (f"Poisson {SERVE_RATE:g} req/s for {seconds:g} s, {n} requests, plates and "
                      f"stiffened boxes, size classes 0..{SERVE_MAX_CLASS} (5e3..2.5e4 DOF); "
                      f"latency = completion - arrival; slot groups of 8/4/2/1 per class reserved "

@@ -58,13 +58,19 @@ T_MIN = 0.0015
 
 
 def tune_class_fill(mesh, ordering, rtol=1e-8, margin=2):
-    """ILU fill level of a size class: the batch autotuner's choice at the
-    thinnest thickness any request of the class can carry (the hardest case
-    for block ILU on shells), plus a margin, so every request converges."""
+    """ILU fill level of a size class: the autotuner's choice for the class
+    mesh alone at the thinnest thickness any request of the class can carry
+    (the hardest case for block ILU on shells), plus a margin where the
+    factor's rows still fit the triangular sweep, so every request
+    converges."""
     import dataclasses
     m = dataclasses.replace(mesh, thick=np.full(mesh.num_elements, T_MIN))
-    return BatchSolver([m], ordering=ordering, tune=True, rtol=rtol,
-                       build=False).fills[0] + margin
+    bs = BatchSolver([m], ordering=ordering, tune=True, rtol=rtol, build=False,
+                     objective="problem")
+    k = bs.fills[0]
+    if k >= L.GF_FILL_FULL:
+        return k
+    return fit_fill(bs.asms[0], k + margin, "fp32")
 
 
 @dataclass
@@ -136,6 +142,25 @@ class Group:
         return stats[:len(reqs)]
 
 
+def fit_fill(asm, fill, precision):
+    """The highest fill level <= `fill` whose factor rows fit the triangular
+    sweep's shared-memory stage for factors of `precision` (FP64 factor rows
+    take twice the bytes of FP32 ones, so a fill tuned with FP32 factors may
+    not fit with FP64 factors)."""
+    if fill >= L.GF_FILL_FULL:
+        return fill
+    k = fill
+    while k > 0:
+        try:
+            ILUk_Preconditioner(asm, k, precision)
+            return k
+        except L.GpuFemError as e:
+            if e.status != L.GF_INVALID_ARG:
+                raise
+            k -= 1
+    return 0
+
+
 class SizeClass:
     """Device-resident mesh, ordering, pattern and scatter schedule of one size
     class, with slot groups reserved at warm-up (nothing is allocated while
@@ -145,7 +170,8 @@ class SizeClass:
         self.family, self.k = family, k
         self.mesh = class_mesh(family, dof)
         self.ordering, self.asm = choose_ordering(self.mesh)
-        self.fill = fill if fill is not None else tune_class_fill(self.mesh, self.ordering, rtol)
+        fill = fill if fill is not None else tune_class_fill(self.mesh, self.ordering, rtol)
+        self.fill = fit_fill(self.asm, fill, precision)
         self.precision = precision
         self.groups = []       # reserved
         self.free = []         # groups not running
