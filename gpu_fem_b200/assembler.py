@@ -363,7 +363,7 @@ class ILUk_Preconditioner:
     def layout(self):
         v = [C.c_int32() for _ in range(5)]
         check(L.lib().gf_precond_layout(self.h, *[C.byref(x) for x in v]), "layout")
-        return {"nsplit_L": v[0].value, "nsplit_U": v[1].value, "fac_split": v[2].value,
+        return {"nsplit_L": v[0].value, "nsplit_U": v[1].value, "fac_ctas": v[2].value,
                 "chunks_L": v[3].value, "chunks_U": v[4].value}
 
     def status(self):

@@ -159,7 +159,7 @@ struct ProbDev {
   const int32_t* pdiag;
   double* LU64;              // factor in ILU-pattern order (FP64)
   int nlevL, nlevU;          // triangular levels
-  int fac_split;             // factor each level's rows on both CTAs of a cluster
+  int32_t* done;             // per row: epoch of the factorization that finished it
   const int32_t* levLptr;    // rows grouped by lower level (factorization order)
   const int32_t* levLrows;
   TriDesc L, U;              // chunk streams of the factor for the sweeps

@@ -22,6 +22,7 @@
 // aligned to each problem's own vector, with per-problem Arnoldi states, so
 // a problem's iterates are bitwise identical alone and inside any batch.
 #include <algorithm>
+#include <atomic>
 #include <array>
 #include <chrono>
 #include <cmath>
@@ -251,18 +252,37 @@ __device__ void inv6_warp(double* M, double* Inv, int lane, SweepCtl* ctl, int r
 
 // IKJ block ILU on each problem's ILU pattern (FP64, in place): lower blocks
 // become L_ik = A_ik U_kk^{-1}, the diagonal block is replaced by U_ii^{-1}.
-// One CTA per problem walks the levels of the lower-triangular DAG; the
-// rows of a level are independent, one warp per row, and levels are
-// separated by __syncthreads() (block-scope visibility of global writes).
+// One warp factors one row. The row's values are staged in the warp's slice
+// of shared memory (rows up to kFacVals blocks; longer rows are updated in
+// global memory), so the read-modify-writes of the sequential steps cost a
+// shared-memory latency, and the row is written back whole when it is final.
 // Within a row the steps k (its lower blocks, ascending) are sequential; a
 // step's updates A_ij -= L_ik U_kj over j in U(k) are spread over the lanes
-// (lane = block slot b < 5, column c < 6; 2 slot batches in flight), and
-// the column lists and U_kj values of a batch are loaded together with
-// A_ik and U_kk^{-1} so a step costs about two memory latencies. Each row's
-// column indices are staged in shared memory for the searches j -> slot.
-constexpr int kFacWarps = 16;
+// (lane = block slot b < 5, column c < 6; 2 slot batches in flight). The
+// column lists and U_kj values of a step's first batch (final rows in
+// global memory) are loaded together with U_kk^{-1}. Each row's column
+// indices are staged for the searches j -> slot.
+//
+// Scheduling is dataflow, not level-synchronous: the warps of the CTAs a
+// problem is given take its rows in factorization order (ascending lower
+// level) from a per-problem counter, and step k of row i waits only until
+// row k is final (its flag done[k] equals the launch's epoch, stored with
+// release after all of row k's values). Rows of later levels therefore run
+// while the rows they do not read are still being factored, and a row's
+// early steps overlap the end of the rows it reads last. Every row that a
+// warp waits for has a lower level, so it was taken earlier by a warp that
+// is running; the waits end whatever the CTAs' residency. Each wait is still
+// bounded: the first that runs out sets ST_TIMEOUT, which ends the others.
+constexpr int kFacWarps = 8;
 constexpr int kFacRow = 256;    // row blocks whose columns are staged in shared memory
-constexpr int kFacBatch = 2;    // update passes of 5 blocks in flight per lane
+constexpr int kFacVals = 80;    // row blocks whose values are staged in shared memory
+constexpr int kFacPass = 6;     // passes of 5 U(k) blocks loaded at the start of a step
+constexpr int kFacBatch = 2;    // passes of 5 blocks in flight per lane beyond those
+constexpr int kFacMap = 1024;   // column span of a row whose column -> slot map is kept
+// per warp: values, L_ik, the diagonal block and its inverse, columns, map
+constexpr size_t kFacWarpSmem = sizeof(double) * (36 * kFacVals + 3 * 36) +
+                                sizeof(int32_t) * kFacRow + sizeof(int16_t) * kFacMap;
+constexpr size_t kFacSmem = kFacWarps * kFacWarpSmem;
 
 __device__ __forceinline__ int find_col(const int32_t* c, int lo, int hi, int j) {
   const int end = hi;
@@ -276,156 +296,265 @@ __device__ __forceinline__ int find_col(const int32_t* c, int lo, int hi, int j)
   return (lo < end && c[lo] == j) ? lo : -1;
 }
 
-// Problems with many rows per level factor each level on both CTAs of a
-// thread-block cluster (rows alternate between their warps); the CTAs meet
-// after every level on a pair of mbarriers (remote arrive with release,
-// bounded wait with acquire, at cluster scope) and end on a cluster barrier
-// that every path reaches. Other problems run on the first CTA alone.
-__global__ void __launch_bounds__(kFacWarps * 32) bfactor_kernel(const ProbDev* __restrict__ P,
-                                                                SweepCtl* ctl) {
-  __shared__ double sL[kFacWarps][36];
-  __shared__ double sM[kFacWarps][36];
-  __shared__ double sI[kFacWarps][36];
-  __shared__ int32_t sC[kFacWarps][kFacRow];
-  __shared__ uint64_t fbar[2];  // the partner's "level done" arrivals, alternating
-  __shared__ int fabort;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  const int b = lane / 6, c = lane % 6;  // update slot and column (lanes 30, 31 idle)
-  const unsigned rank = cluster_rank();
-  const ProbDev d = P[blockIdx.x / kSweepCta];
-  const bool split = d.fac_split != 0;
-  if (!split && rank != 0) return;
-  if (threadIdx.x == 0) {
-    mbar_init(&fbar[0], 1);
-    mbar_init(&fbar[1], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    fabort = 0;
+__device__ __forceinline__ int ld_relaxed_gpu(const int* p) {
+  int v;
+  asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_gpu(int* p, int v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
+// Waits (bounded) until *flag == want, then acquires what its writer
+// released. False when the bound ran out (ST_TIMEOUT set here) or another
+// wait already ran out.
+__device__ bool wait_flag(const int* flag, int want, unsigned long long limit, SweepCtl* ctl) {
+  if (ld_relaxed_gpu(flag) == want) {
+    fence_acq_rel_gpu();
+    return true;
   }
-  if (split)
-    cluster_barrier();
-  else
-    __syncthreads();
-  const unsigned pfbar = split ? cluster_map(smem_u32(fbar), rank ^ 1u) : 0u;
+  const unsigned long long t0 = gtimer();
+  while (true) {
+    if (ld_relaxed_gpu(flag) == want) {
+      fence_acq_rel_gpu();
+      return true;
+    }
+    if (ld_relaxed_gpu(&ctl->status) & ST_TIMEOUT) return false;
+    if (gtimer() - t0 > limit) {
+      atomicOr(&ctl->status, ST_TIMEOUT);
+      return false;
+    }
+  }
+}
+
+// cta_prob[blockIdx.x]: the problem a CTA works on; grab[p]: problem p's row
+// counter (zero at launch).
+__global__ void __launch_bounds__(kFacWarps * 32) bfactor_df(const ProbDev* __restrict__ P,
+                                                            const int32_t* __restrict__ cta_prob,
+                                                            int* __restrict__ grab, int epoch,
+                                                            SweepCtl* ctl) {
+  extern __shared__ __align__(16) unsigned char fsm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  unsigned char* ws = fsm + (size_t)warp * kFacWarpSmem;
+  double* sR = reinterpret_cast<double*>(ws);  // staged row values
+  double* Lb = sR + 36 * kFacVals;             // L_ik of the current step
+  double* sM = Lb + 36;                        // diagonal block (pivoting copy)
+  double* sI = sM + 36;                        // its inverse
+  int32_t* sC = reinterpret_cast<int32_t*>(sI + 36);
+  int16_t* sMap = reinterpret_cast<int16_t*>(sC + kFacRow);  // column - base -> slot - r0, or -1
+  for (int t = lane; t < kFacMap; t += 32) sMap[t] = -1;
+  __syncwarp();
+  const int b = lane / 6, c = lane % 6;  // update slot and column (lanes 30, 31 idle)
+  const int prob = cta_prob[blockIdx.x];
+  const ProbDev d = P[prob];
+  int* counter = grab + prob;
+  int* done = d.done;
   const unsigned long long wlim = g_wait_ns;
-  const bool arrive = !(g_skip_meet && rank == 1);
-  const int wbase = split ? (int)rank * nw + warp : warp, wstride = split ? 2 * nw : nw;
+  const bool skip_first = g_skip_meet != 0;  // failure injection: row 0 of the order never published
   const int32_t* rowp = d.prowp;
   const int32_t* cols = d.pcols;
   const int32_t* diag = d.pdiag;
   double* LU = d.LU64;
-  double* Lb = sL[warp];
-  for (int lev = 0; lev < d.nlevL; lev++) {
-    for (int idx = d.levLptr[lev] + wbase; idx < d.levLptr[lev + 1]; idx += wstride) {
-      const int i = d.levLrows[idx];
-      const int r0 = rowp[i], r1 = rowp[i + 1], di = diag[i], len = r1 - r0;
-      const bool staged = len <= kFacRow;
-      const int32_t* rc = staged ? sC[warp] - r0 : cols;  // rc[kp] = column of slot kp
-      if (staged)
-        for (int t = lane; t < len; t += 32) sC[warp][t] = cols[r0 + t];
+  int idx = lane == 0 ? atomicAdd(counter, 1) : 0;
+  idx = __shfl_sync(0xffffffffu, idx, 0);
+  bool live = true;
+  while (idx < d.n && live) {
+    const int nidx = lane == 0 ? atomicAdd(counter, 1) : 0;  // the next row, in flight meanwhile
+    const int i = d.levLrows[idx];
+    const int r0 = rowp[i], r1 = rowp[i + 1], di = diag[i], len = r1 - r0;
+    const bool cstaged = len <= kFacRow;
+    const bool vstaged = len <= kFacVals;
+    const int32_t* rc = cstaged ? sC - r0 : cols;  // rc[kp] = column of slot kp
+    double* R = vstaged ? sR - 36 * (size_t)r0 : LU;  // R[36 kp + e] = entry e of slot kp
+    if (cstaged)
+      for (int t = lane; t < len; t += 32) sC[t] = cols[r0 + t];
+    // column -> slot map of the row when its column span fits (binary
+    // searches otherwise)
+    const int cbase = cols[r0], span = cols[r1 - 1] - cbase + 1;
+    const bool mapped = span <= kFacMap;
+    if (mapped)
+      for (int t = lane; t < len; t += 32) sMap[cols[r0 + t] - cbase] = (int16_t)t;
+    if (vstaged) {
+      // eight loads in flight per lane
+      const double* src = LU + 36 * (size_t)r0;
+      const int nv = 36 * len;
+      for (int t0 = 0; t0 < nv; t0 += 256) {
+        double v[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          const int t = t0 + 32 * q + lane;
+          v[q] = t < nv ? src[t] : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          const int t = t0 + 32 * q + lane;
+          if (t < nv) sR[t] = v[q];
+        }
+      }
+    }
+    __syncwarp();
+    unsigned ready = 0;  // bit s: the row of step (window start + s) is final
+    for (int kp = r0; kp < di; kp++) {
+      const int s = (kp - r0) & 31;
+      if (s == 0) {
+        // the flags of the next 32 steps, one per lane; a lane that sees
+        // its row final acquires it for the warp (the warp barrier below
+        // orders that acquire before every lane's later loads)
+        const int q = kp + lane;
+        const int f = q < di ? (ld_relaxed_gpu(done + rc[q]) == epoch) : 1;
+        fence_acq_rel_gpu();
+        ready = __ballot_sync(0xffffffffu, f);
+        __syncwarp();
+      }
+      const int k = rc[kp];
+      if (!((ready >> s) & 1u)) {
+        int ok = lane == 0 ? (int)wait_flag(done + k, epoch, wlim, ctl) : 0;
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        __syncwarp();
+        if (!ok) {
+          live = false;
+          break;
+        }
+      }
+      const int u0 = diag[k] + 1, u1 = rowp[k + 1];
+      // loads that do not depend on this row's earlier steps, all in flight
+      // together: the first kFacPass x 5 blocks of U(k) (columns and values)
+      // and U_kk^{-1}
+      int jc[kFacPass];
+      double u[kFacPass][6];
+#pragma unroll
+      for (int q = 0; q < kFacPass; q++) {
+        const int jp = u0 + 5 * q + b;
+        const bool in = lane < 30 && jp < u1;
+        jc[q] = in ? cols[jp] : -1;
+#pragma unroll
+        for (int m = 0; m < 6; m++) u[q][m] = in ? LU[36 * (size_t)jp + 6 * m + c] : 0.0;
+      }
+      const double* Ukk = LU + 36 * (size_t)diag[k];
+      double* Aik = R + 36 * (size_t)kp;
+      double s0 = 0.0, s1 = 0.0;
+      {
+        const int r = lane / 6, cc = lane % 6;
+#pragma unroll
+        for (int m = 0; m < 6; m++) s0 = fma(Aik[6 * r + m], Ukk[6 * m + cc], s0);
+        if (lane < 4) {
+          const int r2 = (lane + 32) / 6, c2 = (lane + 32) % 6;
+#pragma unroll
+          for (int m = 0; m < 6; m++) s1 = fma(Aik[6 * r2 + m], Ukk[6 * m + c2], s1);
+        }
+      }
       __syncwarp();
-      for (int kp = r0; kp < di; kp++) {
-        const int k = rc[kp];
-        const int u0 = diag[k] + 1, u1 = rowp[k + 1];
-        // loads that do not depend on this row's earlier steps: the first
-        // batch of U(k) columns and values, U_kk^{-1}
-        int jc[kFacBatch];
-        double u[kFacBatch][6];
+      Lb[lane] = s0;
+      Aik[lane] = s0;
+      if (lane < 4) {
+        Lb[32 + lane] = s1;
+        Aik[32 + lane] = s1;
+      }
+      __syncwarp();
+      {
+        // targets of the prefetched blocks (distinct slots of this row), then
+        // all their reads before any write
+        int tp[kFacPass];
+#pragma unroll
+        for (int q = 0; q < kFacPass; q++) {
+          if (mapped) {
+            const int off = jc[q] - cbase;
+            const int m = (jc[q] >= 0 && off < span) ? sMap[off] : -1;
+            tp[q] = m >= 0 ? r0 + m : -1;
+          } else {
+            tp[q] = jc[q] >= 0 ? find_col(rc, kp + 1, r1, jc[q]) : -1;
+          }
+        }
+        double lb[36];  // L_ik in registers for the updates
+#pragma unroll
+        for (int t = 0; t < 36; t++) lb[t] = Lb[t];
+        double a[kFacPass][6];
+#pragma unroll
+        for (int q = 0; q < kFacPass; q++)
+#pragma unroll
+          for (int r = 0; r < 6; r++) a[q][r] = tp[q] >= 0 ? R[36 * (size_t)tp[q] + 6 * r + c] : 0.0;
+#pragma unroll
+        for (int q = 0; q < kFacPass; q++)
+          if (tp[q] >= 0) {
+#pragma unroll
+            for (int r = 0; r < 6; r++) {
+              double sacc = 0.0;
+#pragma unroll
+              for (int m = 0; m < 6; m++) sacc = fma(lb[6 * r + m], u[q][m], sacc);
+              R[36 * (size_t)tp[q] + 6 * r + c] = a[q][r] - sacc;
+            }
+          }
+      }
+      // the rest of U(k) (rows longer than the prefetch), kFacBatch passes at a time
+      for (int jb = u0 + 5 * kFacPass; jb < u1; jb += 5 * kFacBatch) {
+        int jt[kFacBatch];
+        double v[kFacBatch][6];
 #pragma unroll
         for (int q = 0; q < kFacBatch; q++) {
-          // the values do not wait for the column index (both in flight)
-          const int jp = u0 + 5 * q + b;
+          const int jp = jb + 5 * q + b;
           const bool in = lane < 30 && jp < u1;
-          jc[q] = in ? cols[jp] : -1;
+          jt[q] = in ? cols[jp] : -1;
 #pragma unroll
-          for (int m = 0; m < 6; m++) u[q][m] = in ? LU[36 * (size_t)jp + 6 * m + c] : 0.0;
+          for (int m = 0; m < 6; m++) v[q][m] = in ? LU[36 * (size_t)jp + 6 * m + c] : 0.0;
         }
-        const double* Ukk = LU + 36 * (size_t)diag[k];
-        double* Aik = LU + 36 * (size_t)kp;
-        double s0 = 0.0, s1 = 0.0;
-        {
-          const int r = lane / 6, cc = lane % 6;
+        int tp[kFacBatch];
 #pragma unroll
-          for (int m = 0; m < 6; m++) s0 = fma(Aik[6 * r + m], Ukk[6 * m + cc], s0);
-          if (lane < 4) {
-            const int r2 = (lane + 32) / 6, c2 = (lane + 32) % 6;
-#pragma unroll
-            for (int m = 0; m < 6; m++) s1 = fma(Aik[6 * r2 + m], Ukk[6 * m + c2], s1);
+        for (int q = 0; q < kFacBatch; q++) {
+          if (mapped) {
+            const int off = jt[q] - cbase;
+            const int m = (jt[q] >= 0 && off < span) ? sMap[off] : -1;
+            tp[q] = m >= 0 ? r0 + m : -1;
+          } else {
+            tp[q] = jt[q] >= 0 ? find_col(rc, kp + 1, r1, jt[q]) : -1;
           }
         }
-        __syncwarp();
-        Lb[lane] = s0;
-        Aik[lane] = s0;
-        if (lane < 4) {
-          Lb[32 + lane] = s1;
-          Aik[32 + lane] = s1;
-        }
-        __syncwarp();
-        for (int jb = u0; jb < u1; jb += 5 * kFacBatch) {
-          if (jb != u0) {
+        double a[kFacBatch][6];
 #pragma unroll
-            for (int q = 0; q < kFacBatch; q++) {
-              const int jp = jb + 5 * q + b;
-              const bool in = lane < 30 && jp < u1;
-              jc[q] = in ? cols[jp] : -1;
+        for (int q = 0; q < kFacBatch; q++)
 #pragma unroll
-              for (int m = 0; m < 6; m++) u[q][m] = in ? LU[36 * (size_t)jp + 6 * m + c] : 0.0;
+          for (int r = 0; r < 6; r++) a[q][r] = tp[q] >= 0 ? R[36 * (size_t)tp[q] + 6 * r + c] : 0.0;
+#pragma unroll
+        for (int q = 0; q < kFacBatch; q++)
+          if (tp[q] >= 0) {
+#pragma unroll
+            for (int r = 0; r < 6; r++) {
+              double sacc = 0.0;
+#pragma unroll
+              for (int m = 0; m < 6; m++) sacc = fma(Lb[6 * r + m], v[q][m], sacc);
+              R[36 * (size_t)tp[q] + 6 * r + c] = a[q][r] - sacc;
             }
           }
-          int tp[kFacBatch];
-#pragma unroll
-          for (int q = 0; q < kFacBatch; q++)
-            tp[q] = jc[q] >= 0 ? find_col(rc, kp + 1, r1, jc[q]) : -1;
-          double a[kFacBatch][6];
-#pragma unroll
-          for (int q = 0; q < kFacBatch; q++)
-            if (tp[q] >= 0)
-#pragma unroll
-              for (int r = 0; r < 6; r++) a[q][r] = LU[36 * (size_t)tp[q] + 6 * r + c];
-#pragma unroll
-          for (int q = 0; q < kFacBatch; q++)
-            if (tp[q] >= 0) {
-#pragma unroll
-              for (int r = 0; r < 6; r++) {
-                double s = 0.0;
-#pragma unroll
-                for (int m = 0; m < 6; m++) s = fma(Lb[6 * r + m], u[q][m], s);
-                LU[36 * (size_t)tp[q] + 6 * r + c] = a[q][r] - s;
-              }
-            }
-        }
-        __syncwarp();
-      }
-      double* Dii = LU + 36 * (size_t)di;
-      for (int t = lane; t < 36; t += 32) sM[warp][t] = Dii[t];
-      __syncwarp();
-      inv6_warp(sM[warp], sI[warp], lane, ctl, d.off + i);
-      for (int t = lane; t < 36; t += 32) {
-        const double v = sI[warp][t];
-        if (!isfinite(v)) {
-          atomicOr(&ctl->status, ST_ZERO_PIVOT);
-          atomicCAS(&ctl->pivot, 0, d.off + i + 1);
-        }
-        Dii[t] = v;
       }
       __syncwarp();
     }
-    __syncthreads();
-    if (split) {
-      // both CTAs' rows of this level are final before either starts the next
-      if (threadIdx.x == 0) {
-        const unsigned slot = (unsigned)(lev & 1);
-        if (arrive) mbar_arrive_remote(pfbar + 8u * slot);
-        if (!mbar_wait_cluster(&fbar[slot], (unsigned)((lev >> 1) & 1), wlim)) {
-          fabort = 1;
-          atomicOr(&ctl->status, ST_TIMEOUT);
-        }
+    if (!live) break;
+    double* Dii = R + 36 * (size_t)di;
+    for (int t = lane; t < 36; t += 32) sM[t] = Dii[t];
+    __syncwarp();
+    inv6_warp(sM, sI, lane, ctl, d.off + i);
+    for (int t = lane; t < 36; t += 32) {
+      const double v = sI[t];
+      if (!isfinite(v)) {
+        atomicOr(&ctl->status, ST_ZERO_PIVOT);
+        atomicCAS(&ctl->pivot, 0, d.off + i + 1);
       }
-      __syncthreads();
-      if (fabort) break;
+      Dii[t] = v;
     }
+    __syncwarp();
+    if (vstaged) {
+      double* dst = LU + 36 * (size_t)r0;
+      for (int t = lane; t < 36 * len; t += 32) dst[t] = sR[t];
+    }
+    if (mapped)
+      for (int t = lane; t < len; t += 32) sMap[cols[r0 + t] - cbase] = -1;
+    // publish: every lane's stores of the row reach device scope before the
+    // flag (release) says the row is final
+    __threadfence();
+    __syncwarp();
+    if (lane == 0 && !(skip_first && idx == 0)) st_release_gpu(done + i, epoch);
+    idx = __shfl_sync(0xffffffffu, nidx, 0);
   }
-  // no CTA leaves while its partner may still arrive on its barriers
-  if (split) cluster_barrier();
 }
 
 __global__ void scatter_values_kernel(int nA, const int32_t* __restrict__ map,
@@ -1329,6 +1458,8 @@ struct gf_precond {
   std::vector<int32_t> lvL, lvU;
   DevBuf<int32_t> d_rowp, d_cols, d_diag, d_amap;
   DevBuf<int32_t> d_levLptr, d_levLrows;  // factorization order
+  DevBuf<int32_t> d_done;                  // per row: epoch of the factorization that finished it
+  long long fwork = 0;                     // block updates of one factorization
   DevBuf<double> d_lu;
   struct Tri {
     int nch = 0, stage = 0, capb = 0, capr = 0, nsplit = 1;
@@ -1705,6 +1836,8 @@ struct gf_batch {
   DevBuf<double> d_tmp, d_b, d_x;
   int nchunks = 0;
   DevBuf<int32_t> d_cprob, d_pstart;
+  int fac_grid = 0;                  // CTAs of the dataflow factorization
+  DevBuf<int32_t> d_fcta, d_fgrab;   // problem of each CTA; per-problem row counters
   DevBuf<int64_t> d_clo, d_chi;
   DevBuf<PermEntry> d_perm_b, d_perm_x, d_perm_out;
   int m = 0;
@@ -1716,16 +1849,47 @@ struct gf_batch {
 
 namespace gf {
 
-// two CTAs per level pay off once a level has more rows than one CTA's warps
-static int fac_split_of(const gf_precond* p) {
-  return p->pat.n > kFacWarps * std::max(p->nlevL, 1) ? 1 : 0;
-}
-
 static int sm_count() {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   return sms;
+}
+
+// CTAs of the dataflow factorization for one problem given `budget` CTAs for
+// it: at least one, at most one per 32 rows (four rows per warp) and 128.
+static int fac_ctas_cap(const gf_precond* p, int budget) {
+  return std::max(1, std::min({budget, 128, p->pat.n / (4 * kFacWarps)}));
+}
+// A preconditioner factored alone gets the whole GPU (one CTA per SM).
+static int fac_ctas_alone(const gf_precond* p) { return fac_ctas_cap(p, sm_count()); }
+
+// Spreads one CTA per SM over the batch's problems in proportion to their
+// block updates (largest remainders first), within each problem's cap;
+// fills cta_prob with the problem of every CTA.
+static void fac_plan(const std::vector<gf_precond*>& pcs, std::vector<int>& ctas,
+                     std::vector<int32_t>& cta_prob) {
+  const int np = (int)pcs.size(), total = std::max(sm_count(), np);
+  double W = 0.0;
+  for (auto* p : pcs) W += (double)std::max<long long>(p->fwork, 1);
+  ctas.assign(np, 1);
+  std::vector<std::pair<double, int>> rem;
+  int used = 0;
+  for (int k = 0; k < np; k++) {
+    const double want = total * (double)std::max<long long>(pcs[k]->fwork, 1) / W;
+    const int cap = fac_ctas_cap(pcs[k], total);
+    ctas[k] = std::max(1, std::min(cap, (int)want));
+    used += ctas[k];
+    if (ctas[k] < cap) rem.push_back({want - ctas[k], k});
+  }
+  std::sort(rem.begin(), rem.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+  for (size_t q = 0; q < rem.size() && used < total; q++) {
+    ctas[rem[q].second]++;
+    used++;
+  }
+  cta_prob.clear();
+  for (int k = 0; k < np; k++)
+    for (int c = 0; c < ctas[k]; c++) cta_prob.push_back(k);
 }
 
 // Descriptor table (rebuilt when a buffer such as the FP32 matrix copy is
@@ -1747,7 +1911,7 @@ static gf_status upload_desc(gf_batch* B) {
     d.pdiag = p->d_diag.p;
     d.LU64 = p->d_lu.p;
     d.nlevL = p->nlevL;
-    d.fac_split = fac_split_of(p);
+    d.done = p->d_done.p;
     d.nlevU = p->nlevU;
     d.levLptr = p->d_levLptr.p;
     d.levLrows = p->d_levLrows.p;
@@ -1798,6 +1962,14 @@ static gf_status batch_build(gf_batch* B) {
     if (e == cudaSuccess) e = x;
   };
   up(B->d_desc.alloc(np));
+  {
+    std::vector<int> ctas;
+    std::vector<int32_t> cta_prob;
+    fac_plan(B->pcs, ctas, cta_prob);
+    B->fac_grid = (int)cta_prob.size();
+    up(B->d_fcta.upload(cta_prob));
+    up(B->d_fgrab.alloc(np));
+  }
   up(B->d_row_prob.upload(row_prob));
   up(B->d_ctl.alloc(1));
   if (e == cudaSuccess) up(cudaMemset(B->d_ctl.p, 0, sizeof(SweepCtl)));
@@ -2018,21 +2190,20 @@ static gf_status batch_factor(gf_batch* B, cudaStream_t st) {
   }
   GF_CHECK_LAUNCH();
   {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)(B->np * kSweepCta));
-    cfg.blockDim = dim3(kFacWarps * 32);
-    cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = kSweepCta;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    const ProbDev* desc = B->d_desc.p;
-    SweepCtl* ctl = B->d_ctl.p;
+    // a fresh epoch per launch: flags left by earlier factorizations (of any
+    // batch holding these preconditioners) never equal it
+    static std::atomic<int> epochs{0};
+    int epoch = ++epochs;
+    if (epoch <= 0) {
+      epochs = 1;
+      epoch = 1;
+    }
+    GF_CUDA(cudaMemsetAsync(B->d_fgrab.p, 0, sizeof(int32_t) * B->np, st));
     ::gf::count_launch();
-    GF_CUDA(cudaLaunchKernelEx(&cfg, bfactor_kernel, desc, ctl));
+    GF_CUDA(cudaFuncSetAttribute(bfactor_df, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kFacSmem));
+    bfactor_df<<<(unsigned)B->fac_grid, kFacWarps * 32, kFacSmem, st>>>(
+        B->d_desc.p, B->d_fcta.p, B->d_fgrab.p, epoch, B->d_ctl.p);
   }
   GF_CHECK_LAUNCH();
   for (int k = 0; k < B->np; k++) {
@@ -2405,6 +2576,16 @@ gf_status gf_precond_create_ex(gf_assembler* a, int32_t fill_level, int32_t prec
   up(p->d_levLptr.upload(lptr));
   up(p->d_levLrows.upload(lrows));
   up(p->d_lu.alloc((size_t)36 * p->pat.nnz()));
+  up(p->d_done.alloc((size_t)n));
+  if (e == cudaSuccess) up(cudaMemset(p->d_done.p, 0, sizeof(int32_t) * (size_t)n));
+  // block updates of one factorization: per step (i, k) the block L_ik and
+  // one update per block of U(k)
+  p->fwork = 0;
+  for (int i = 0; i < n; i++)
+    for (int kp = p->pat.rowp[i]; kp < diag[i]; kp++) {
+      const int k = p->pat.cols[kp];
+      p->fwork += p->pat.rowp[k + 1] - diag[k];
+    }
   for (int w = 0; w < 2 && e == cudaSuccess; w++) {
     bool df = false;
     if (sweep == GF_SWEEP_DATAFLOW) e = build_df(p, diag, w == 1, &df);
@@ -2452,11 +2633,11 @@ gf_status gf_precond_info(const gf_precond* p, int32_t* nnzb, int32_t* nl, int32
 }
 
 gf_status gf_precond_layout(const gf_precond* p, int32_t* nsplit_L, int32_t* nsplit_U,
-                            int32_t* fac_split, int32_t* chunks_L, int32_t* chunks_U) {
+                            int32_t* fac_ctas, int32_t* chunks_L, int32_t* chunks_U) {
   if (!p) return GF_INVALID_ARG;
   if (nsplit_L) *nsplit_L = p->tri[0].nsplit;
   if (nsplit_U) *nsplit_U = p->tri[1].nsplit;
-  if (fac_split) *fac_split = fac_split_of(p);
+  if (fac_ctas) *fac_ctas = fac_ctas_alone(p);
   if (chunks_L) *chunks_L = p->tri[0].nch;
   if (chunks_U) *chunks_U = p->tri[1].nch;
   return GF_OK;

@@ -274,14 +274,15 @@ gf_status gf_precond_apply_noalloc(gf_precond* p, const double* d_r, double* d_z
  * errors, include/cuda_utils.h:35-43). */
 gf_status gf_precond_status(gf_precond* p, void* stream);
 /* How the triangular work of this preconditioner is laid out on the GPU:
- * CTAs that share each sweep chunk's rows (1 or 2) for L and U, whether the
- * factorization splits each level's rows over a 2-CTA cluster, and the
- * number of chunks of each triangle (a chunk holds rows of one level; a
+ * CTAs that share each sweep chunk's rows (1 or 2) for L and U, the CTAs the
+ * dataflow factorization runs on when this preconditioner is factored alone
+ * (1 to 128; in a batch the SMs are shared out by the problems' block
+ * updates), and the number of chunks of each triangle (a chunk holds rows of one level; a
  * level with more blocks than a chunk's stage spans several). Any pointer
  * may be NULL. No reference counterpart (cuSPARSE's bsrsv2 level analysis is
  * internal). */
 gf_status gf_precond_layout(const gf_precond* p, int32_t* nsplit_L, int32_t* nsplit_U,
-                            int32_t* fac_split, int32_t* chunks_L, int32_t* chunks_U);
+                            int32_t* fac_ctas, int32_t* chunks_L, int32_t* chunks_U);
 /* Pattern, level count and factor copy for checking. rowPtr/colPtr may be
  * NULL; values receives nnzb_pc*36 entries with the diagonal blocks holding
  * U_ii^{-1}. */
@@ -371,11 +372,13 @@ gf_status gf_batch_solve(gf_batch* b, const double* const* d_b, double* const* d
 
 /* ---- failure injection for tests ------------------------------------- */
 /* Sets, on the current device, the bound of the device-side waits that end
- * when a bulk copy lands or a partner CTA arrives (wait_ns; 0 restores the
- * default of 2 s), and whether CTA rank 1 of every split triangle or
- * factorization skips its arrivals on the partner's meeting barriers
- * (skip_meetings != 0), which makes the partner's bounded wait run out so
- * that the launch reports GF_TIMEOUT. The waits that drain a CTA's own copies
+ * when a bulk copy lands, a partner CTA arrives or a row that is read is
+ * final (wait_ns; 0 restores the default of 2 s), and whether the kernels
+ * skip publishing (skip_meetings != 0): CTA rank 1 of every split triangle
+ * skips its arrivals on the partner's meeting barriers, the factorization
+ * never publishes the first row of its order and the dataflow sweep's warp
+ * 0 never publishes its rows, which makes the bounded waits run out so that
+ * the launch reports GF_TIMEOUT. The waits that drain a CTA's own copies
  * in flight keep the 2 s bound, and both CTAs of a cluster still meet on the
  * final cluster barrier, so nothing hangs. Process-wide for the device: set
  * it only while no other work of this library runs there, and restore it

@@ -3,9 +3,9 @@ the triangular sweeps, the paths the large batched problems run.
 
 Case: 256 x 128 clamped plate, t = 2 mm, natural node ordering, ILU(6):
 33,153 block rows and 1,281 levels per triangle, about 26 rows and 405 (L) /
-431 (U) blocks per level. The factorization splits every level's rows over a
-2-CTA cluster (more than 16 rows a level). The sweeps are checked in both
-kernels:
+431 (U) blocks per level. The dataflow factorization runs on 128 CTAs whose
+warps take rows in level order and wait per step for the rows they read.
+The sweeps are checked in both kernels:
 - level-synchronous (the default): both sweeps split every chunk over the
   two CTAs (more than 200 blocks a level), and with FP64 factors each level
   spans two chunks (a split FP64 chunk holds at most 344 blocks), so near and
@@ -14,7 +14,7 @@ kernels:
   1024-slot result ring that its flow control recycles 32 times per sweep.
 
 Checked, with FP64 and FP32 factor values:
-- the layout really is split (gf_precond_layout);
+- the layout really is split / multi-CTA (gf_precond_layout);
 - the factor's backward error max |(L U - A)_ij| over the ILU pattern is
   within 1e-10 max |A| (sparse block products in the oracle), and two
   factorizations are bitwise equal; ILU(k) is defined by (L U)_ij = A_ij on
@@ -78,7 +78,7 @@ def test_split_factor_and_apply_match_oracle(big, precision, sweep):
     P = ILUk_Preconditioner(big["A"], fill_level=6, precision=precision, sweep=sweep)
     nsL, nsU, fsplit, chL, chU = _layout(P)
     inf = P.info()
-    assert fsplit == 1
+    assert fsplit == 128
     kinds = P.sweeps()
     assert kinds["L"] == kinds["U"] == sweep, kinds
     if sweep == "level":
@@ -156,7 +156,7 @@ def test_split_problems_bitwise_alone_and_in_batch():
     bs = BatchSolver(meshes, ordering="natural", fill=6, tune=False)
     for P in bs.P32:
         lay = _layout(P)
-        assert lay[:3] == [2, 2, 1] and P.sweeps()["L"] == "level", lay
+        assert lay[:2] == [2, 2] and lay[2] == 128 and P.sweeps()["L"] == "level", lay
     stats = bs.step(True)
     assert all(s["rel_residual"] <= 1e-8 for s in stats), stats
     x_mix = [x.cpu().numpy().copy() for x in bs.xs]

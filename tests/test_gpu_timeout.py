@@ -1,13 +1,16 @@
 """Bounded device-side waits report GF_TIMEOUT and leave the context usable.
 
-The split factorization and the split (level-synchronous) sweeps meet the
-partner CTA of their cluster once per level / chunk on mbarriers with
-bounded waits; the dataflow sweep waits, bounded, for the result tags of the
-rows each row multiplies. The tests shorten the bound to 200 us and switch
-on gf_test_set_waits' failure injection: CTA rank 1 skips its meeting
+The dataflow factorization waits, bounded, for the completion flag of every
+row a step reads; the split (level-synchronous) sweeps meet the partner CTA
+of their cluster once per chunk on mbarriers with bounded waits; the
+dataflow sweep waits, bounded, for the result tags of the rows each row
+multiplies. The tests shorten the bound to 200 us and switch on
+gf_test_set_waits' failure injection: the factorization never publishes the
+first row of its order, CTA rank 1 of a sweep cluster skips its meeting
 arrivals, and the dataflow sweep's warp 0 never publishes its rows, so the
-waits run out. The launches record a timeout, both CTAs of a cluster still
-meet on the final cluster barrier, every CTA lets its copies in flight land,
+waits run out. The launches record a timeout (the first wait that runs out
+ends the factorization's other waits), both CTAs of a cluster still meet on
+the final cluster barrier, every CTA lets its copies in flight land,
 and the host reads GF_TIMEOUT from gf_precond_factor, gf_precond_status after
 an apply, and gf_gmres_solve. With the default bound restored, the same
 objects factor and solve correctly. No wait is removed, so nothing can hang,
@@ -43,7 +46,7 @@ def test_timeout_reported_and_context_usable(sweep):
     A.add_jacobian(None, K, fuse_bcs=True)
     P = ILUk_Preconditioner(A, fill_level=6, precision="fp64", sweep=sweep)
     lay = P.layout()
-    assert lay["fac_split"] == 1  # the factorization splits each level over two CTAs
+    assert lay["fac_ctas"] == 128  # the dataflow factorization's CTAs
     assert P.sweeps()["L"] == sweep
     if sweep == "level":  # both sweeps split every chunk over two CTAs
         assert (lay["nsplit_L"], lay["nsplit_U"]) == (2, 2)
@@ -57,7 +60,7 @@ def test_timeout_reported_and_context_usable(sweep):
     torch.cuda.synchronize()
     try:
         L.check(lib.gf_test_set_waits(200_000, 1), "set_waits")
-        # split factorization: the level meetings run out
+        # dataflow factorization: the rows that read the unpublished row time out
         with pytest.raises(L.GpuFemError) as err:
             P.factor(K)
         assert err.value.status == L.GF_TIMEOUT
