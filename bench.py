@@ -243,9 +243,9 @@ SWEEP_TRAFFIC = None
 # per row, then the converging k of smallest modelled factor + solve time) on
 # a B200. Both arms run every problem with these, so their configs match;
 # `--tune` re-runs the autotuner and prints the table it finds.
-FILLS = [6, 8, 5, 3, 4, 3, 4, 4, 4, 1, 4, 4, 3, 3, 7, 5, 5, 4, 3, 7, 3, 2, 4, 5, 3, 7, 3, 2, 3, 4,
-         4, 7, 3, 7, 3, 5, 5, 2, 2, 3, 16, 7, 3, 7, 3, 3, 5, 6, 5, 6, 2, 2, 12, 5, 3, 3, 3, 4, 6,
-         16, 2, 2, 3, 5]
+FILLS = [12, 16, 12, 7, 6, 6, 10, 8, 12, 5, 8, 7, 10, 6, 12, 12, 10, 8, 8, 12, 12, 6, 12, 10, 6,
+         16, 12, 8, 10, 12, 12, 12, 5, 12, 5, 10, 8, 7, 5, 12, 16, 16, 8, 12, 10, 10, 10, 12, 10,
+         12, 8, 7, 16, 12, 6, 7, 8, 12, 12, 16, 4, 4, 10, 12]
 ORDERS = "n" * 64  # one character per problem: "n" natural, "r" RCM
 
 

@@ -85,18 +85,24 @@ ORDERINGS = ("natural", "rcm")
 
 
 def factor_cost_us(nrow, inf):
-    """Critical path of one numeric factorization of a problem (microseconds),
-    fitted to B200 runs of the 64-plate batch. The factorization walks its
-    lower levels in rounds of one row per warp (16 warps, or 32 when levels
-    average more than 16 rows and two CTAs share them); a row's steps are
-    sequential and each updates about one row length of blocks, so a row
-    costs ~0.35 us x (lower blocks)^2."""
+    """One numeric factorization of a problem (microseconds), fitted to B200
+    runs of single plates (16^2 to 256^2 elements, fills 1 to 16) on the
+    dataflow factorization. RCM-ordered factors cost ~7.6 us a lower level:
+    a row waits for its last-finishing dependency and then has only a few
+    steps left. In natural order the rows along a grid line depend on their
+    neighbour and run their same-line steps after the previous line's rows,
+    so a level costs more as rows get longer, and the block updates
+    (~nrow x lower x (lower + 1), lower = blocks left of the diagonal per
+    row) spread over the warps add a throughput term."""
     lvl, nnzb = inf["levels_L"], inf["nnzb"]
     lower = max(nnzb - nrow, 0) / (2.0 * nrow)
-    rows_per_level = nrow / max(lvl, 1)
-    warps = 32 if rows_per_level > 16 else 16
-    rounds = max(1, -(-int(rows_per_level) // warps))
-    return lvl * rounds * 0.35 * lower * lower
+    warps = 8 * max(1, min(128, nrow // 32))
+    work = nrow * lower * (lower + 1.0)
+    if inf.get("ordering", "natural") == "rcm":
+        t = 7.65 * lvl + 0.0049 * lvl * lower + 0.003 * lvl * lower * lower - 0.076 * work / warps - 72.0
+    else:
+        t = 12.09 * lvl - 0.572 * lvl * lower + 0.0099 * lvl * lower * lower + 1.68 * work / warps - 394.5
+    return max(t, 20.0)
 
 
 def sweep_cost_us(inf):
@@ -249,7 +255,7 @@ class BatchSolver:
         for j, i in enumerate(todo):
             s = stats[j]
             nrow = self.asms[i].get_num_nodes()
-            inf = dict(P[j].info(), nrow=nrow)
+            inf = dict(P[j].info(), nrow=nrow, ordering=self.orderings[i])
             nlev = inf["levels_L"] + inf["levels_U"]
             ok = s["status"] == L.GF_OK
             log.append((i, k, s["iterations"], s["rel_residual"], nlev, ok))

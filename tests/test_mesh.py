@@ -47,9 +47,9 @@ def test_batch_config4_seeded():
 
 
 def test_step_cost_model_prefers_what_the_kernels_reward():
-    """The autotuner's step model: a longer factor row costs quadratically
-    in the factorization, more levels cost in every GMRES step, and levels
-    big enough for two CTAs are cheaper per block."""
+    """The autotuner's step model: a longer factor row costs more in the
+    factorization, more levels cost in every GMRES step, and levels big
+    enough for two CTAs are cheaper per block."""
     from gpu_fem_b200.batch import step_cost_us
     n = 20000
     short = step_cost_us(n, {"levels_L": 1000, "levels_U": 1000, "nnzb": 20 * n}, 50)
