@@ -106,14 +106,17 @@ def factor_cost_us(nrow, inf):
 
 
 def sweep_cost_us(inf):
-    """Both triangular sweeps of one preconditioner apply (microseconds):
-    ~1.1 us a level plus ~9 ns per block of the level, or ~1.6 us plus
-    ~4.5 ns when levels average more than 200 blocks and two CTAs share
-    them."""
+    """Both triangular sweeps of one preconditioner apply (microseconds),
+    fitted to B200 applies of the batch's plates: ~1.1 us a level plus
+    ~2.3 ns per block of the level on one CTA, or ~1.6 us plus ~1.6 ns when
+    the level's rows outnumber one CTA's warps or its blocks fill the stage
+    and two CTAs share it (meeting once per chunk)."""
     lvl, lvu, nnzb = inf["levels_L"], inf["levels_U"], inf["nnzb"]
-    nrow = inf.get("nrow")
-    blocks = max(nnzb - (nrow or 0), 0) / 2.0 / max(lvl, 1)
-    per_level = 1.6 + 0.0045 * blocks if blocks > 200 else 1.1 + 0.009 * blocks
+    nrow = inf.get("nrow") or 0
+    blocks = max(nnzb - nrow, 0) / 2.0 / max(lvl, 1)
+    rows = nrow / max(lvl, 1)
+    split = rows > 13 or blocks > 380
+    per_level = 1.6 + 0.0016 * blocks if split else 1.1 + 0.0023 * blocks
     return (lvl + lvu) * per_level
 
 

@@ -793,8 +793,9 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
       }
     }
     __syncthreads();
-    // the producer warp (the last) refills the stage chunk c-1 used while
-    // the other warps solve chunk c's rows
+    // the producer warp (the last) refills the stage chunk c-1 used, then
+    // solves rows like the others (it is given a row only when a chunk has
+    // as many rows as the CTA has warps)
     if (issued < T.nch) {
       if (tid == producer) {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -804,7 +805,7 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
     }
     double* wp = ring + 6 * (size_t)ringrows * (c & 1);
     const unsigned pwp = pring + 8u * 6u * (unsigned)ringrows * (unsigned)(c & 1);
-    for (int k = warp; k < nr && warp < nw - 1; k += nw - 1) {
+    for (int k = warp; k < nr; k += nw) {
       const int4 row = ri[k];
       const int i = row.x, rbeg = row.y, rcnt = row.z, gk = row.w;
       const int first = UPPER ? 1 : 0;  // U rows start with U_ii^{-1}
@@ -1496,13 +1497,37 @@ static cudaError_t build_tri(gf_precond* p, const std::vector<int32_t>& diag, bo
     real += cnt(i);
   }
   const int mc4 = (maxc + 3) & ~3;
-  // Levels of more than ~200 blocks on average are split over the two CTAs
-  // of the problem's cluster: measured on B200, a chunk costs ~1.1 us plus
-  // ~4.7 ns a block on one CTA, and ~1.6 us plus ~2.3 ns a block when two
-  // CTAs share it and meet once per chunk.
-  const int nsplit = real > 200ll * std::max(nlev, 1) ? kSweepCta : 1;
   const int base = p->prec == GF_PREC_FP32 ? 416 : 208;
   const int capr = 128;
+  // One CTA or the two CTAs of the problem's cluster per chunk, whichever
+  // the chunk model of B200 clock64 traces makes cheaper: a chunk costs
+  // ~1,000 cycles of copies and barriers plus ~1,900 cycles per round of
+  // rows over the 16 warps of a CTA (a row's latency), and splitting it
+  // adds ~1,450 cycles for the two CTAs' meeting. Splitting pays when levels
+  // have more rows than one CTA's warps or more blocks than its stage.
+  auto model = [&](int ns) {
+    const int cb = ns > 1 ? ns * (std::max(base, ((3 * mc4 + 1) / 2 + 3) & ~3) - mc4)
+                          : std::max(base, mc4);
+    const int cr = ns * capr, warps = kSweepThreads / 32;
+    double cyc = 0.0;
+    int cur = 0, nr = 0;
+    auto close = [&]() {
+      const int per_cta = (nr + ns - 1) / ns;
+      cyc += 1000.0 + (ns > 1 ? 1450.0 : 0.0) + 1900.0 * ((per_cta + warps - 1) / warps);
+      cur = nr = 0;
+    };
+    for (int l = 0; l < nlev; l++) {
+      for (int k = ptr[l]; k < ptr[l + 1]; k++) {
+        const int c = cnt(rows[k]);
+        if (nr > 0 && (cur + c > cb || nr == cr)) close();
+        cur += c;
+        nr++;
+      }
+      if (nr > 0) close();
+    }
+    return cyc;
+  };
+  const int nsplit = model(kSweepCta) < model(1) ? kSweepCta : 1;
   // per CTA: blocks of one half chunk. Split chunks are bounded so that
   // giving each row to the lighter half leaves every half within capb (a
   // half exceeds the mean by at most half a row) and a longest row fits.

@@ -6,10 +6,13 @@ Case: 256 x 128 clamped plate, t = 2 mm, natural node ordering, ILU(6):
 431 (U) blocks per level. The dataflow factorization runs on 128 CTAs whose
 warps take rows in level order and wait per step for the rows they read.
 The sweeps are checked in both kernels:
-- level-synchronous (the default): both sweeps split every chunk over the
-  two CTAs (more than 200 blocks a level), and with FP64 factors each level
-  spans two chunks (a split FP64 chunk holds at most 344 blocks), so near and
-  far x entries cross chunk and CTA boundaries;
+- level-synchronous (the default): with FP32 factors both sweeps split
+  every chunk over the two CTAs (26 rows a level, more than one CTA's 16
+  warps); with FP64 factors a level (~405 blocks) spans two chunks of one
+  CTA (a chunk stage holds 208 FP64 blocks), which the chunk model makes
+  cheaper than splitting, so near and far x entries cross chunk boundaries.
+  A 512 x 128 plate (43 rows, ~670 blocks a level) has FP64 levels split
+  over both CTAs and spanning two split chunks each;
 - dataflow: every row waits only for the rows it multiplies, through a
   1024-slot result ring that its flow control recycles 32 times per sweep.
 
@@ -82,9 +85,11 @@ def test_split_factor_and_apply_match_oracle(big, precision, sweep):
     kinds = P.sweeps()
     assert kinds["L"] == kinds["U"] == sweep, kinds
     if sweep == "level":
-        assert (nsL, nsU) == (2, 2), (nsL, nsU)
-        if precision == "fp64":
-            # levels larger than one split chunk: more chunks than levels
+        if precision == "fp32":
+            assert (nsL, nsU) == (2, 2), (nsL, nsU)
+        else:
+            # one CTA, levels larger than one chunk: more chunks than levels
+            assert (nsL, nsU) == (1, 1), (nsL, nsU)
             assert chL > inf["levels_L"] and chU > inf["levels_U"], (chL, chU, inf)
     else:
         assert kinds["ring_L"] == kinds["ring_U"] == 1024, kinds
@@ -112,6 +117,38 @@ def test_split_factor_and_apply_match_oracle(big, precision, sweep):
         z_ref = po.ilu_apply_dinv(r2, c2, lu_used, r)
         scale = np.abs(z_ref).max()
         assert np.abs(z - z_ref).max() <= 1e-12 * scale, (call, np.abs(z - z_ref).max() / scale)
+
+
+def test_split_multichunk_levels_match_oracle():
+    """512 x 128 plate, natural order, ILU(6), FP64 factors: every level is
+    split over the two CTAs and spans two split chunks; the factor's
+    backward error and the apply against the oracle's triangular solves."""
+    import torch
+    from gpu_fem_b200.assembler import ElementAssembler, ILUk_Preconditioner, createBsrMat
+    from oracle import pyoracle as po
+    mesh = _plate(512, 128)
+    A = ElementAssembler.from_mesh(mesh, ordering="natural")
+    K = createBsrMat(A)
+    A.add_jacobian(None, K, fuse_bcs=True)
+    P = ILUk_Preconditioner(A, fill_level=6, precision="fp64", sweep="level")
+    nsL, nsU, _, chL, chU = _layout(P)
+    inf = P.info()
+    assert (nsL, nsU) == (2, 2), (nsL, nsU)
+    assert chL > inf["levels_L"] and chU > inf["levels_U"], (chL, chU, inf)
+    P.factor(K)
+    torch.cuda.synchronize()
+    bd = A.getBsrData()
+    rk, ck, lu = P.get()
+    Ak = po.scatter_to_pattern(bd["rowPtr"], bd["colPtr"], K.values_host(), rk, ck)
+    err, amax = po.ilu_backward_error(rk, ck, lu, Ak, dinv=True)
+    assert err <= 1e-10 * amax, (err, amax)
+    r = np.random.default_rng(12).standard_normal(mesh.num_dof)
+    rt = torch.tensor(r, device="cuda")
+    zt = torch.zeros_like(rt)
+    P.apply(rt, zt)
+    z_ref = po.ilu_apply_dinv(rk, ck, lu, r)
+    scale = np.abs(z_ref).max()
+    assert np.abs(zt.cpu().numpy() - z_ref).max() <= 1e-12 * scale
 
 
 def _superlu(mesh, rowp, cols, vals, perm):
@@ -152,11 +189,12 @@ def test_split_solve_matches_direct_solve(big, precision, sweep):
 def test_split_problems_bitwise_alone_and_in_batch():
     from gpu_fem_b200.assembler import ILUk_Preconditioner
     from gpu_fem_b200.batch import BatchSolver
-    meshes = [_plate(160, 80, 0.002, 1e3), _plate(192, 96, 0.003, 1.4e3)]
+    meshes = [_plate(200, 100, 0.002, 1e3), _plate(240, 96, 0.003, 1.4e3)]
     bs = BatchSolver(meshes, ordering="natural", fill=6, tune=False)
     for P in bs.P32:
         lay = _layout(P)
-        assert lay[:2] == [2, 2] and lay[2] == 128 and P.sweeps()["L"] == "level", lay
+        # at least one triangle split over the cluster's two CTAs
+        assert max(lay[:2]) == 2 and lay[2] == 128 and P.sweeps()["L"] == "level", lay
     stats = bs.step(True)
     assert all(s["rel_residual"] <= 1e-8 for s in stats), stats
     x_mix = [x.cpu().numpy().copy() for x in bs.xs]

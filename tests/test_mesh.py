@@ -59,9 +59,9 @@ def test_step_cost_model_prefers_what_the_kernels_reward():
     assert deeper > short
     more_its = step_cost_us(n, {"levels_L": 1000, "levels_U": 1000, "nnzb": 20 * n}, 100)
     assert more_its > short
-    # per level: one CTA below ~200 blocks, two above (cheaper per block)
-    one = step_cost_us(n, {"levels_L": 100, "levels_U": 100, "nnzb": n + 2 * 100 * 190}, 10)
-    two = step_cost_us(n, {"levels_L": 100, "levels_U": 100, "nnzb": n + 2 * 100 * 400}, 10)
+    # per level: one CTA for small levels, two for large ones (cheaper per block)
+    one = step_cost_us(n, {"levels_L": 2000, "levels_U": 2000, "nnzb": n + 2 * 2000 * 190}, 10)
+    two = step_cost_us(n, {"levels_L": 2000, "levels_U": 2000, "nnzb": n + 2 * 2000 * 400}, 10)
     assert two < 2 * one
 
 

@@ -32,12 +32,13 @@ def _factored(mesh, fill, precision, ordering="rcm", sweep="auto"):
 
 def _case(name):
     """single_cta: 24x12 jittered cantilever, RCM, ILU(2), level-synchronous
-    sweeps on one CTA. split: 160x80 clamped plate, natural ordering, ILU(6),
-    13,041 nodes (below the array's 43,690-node capacity), level-synchronous
-    sweeps that split every chunk over a 2-CTA cluster, so the intermediate
-    vector in the fixed array is written by two CTAs. dataflow: the same
-    plate with the dataflow sweeps (the default kernel)."""
-    plate = M.plate(160, 80, 1.0, 0.5, lambda x, y: 0.002 + 0 * x, "all_edges",
+    sweeps on one CTA. split: 256x128 clamped plate, natural ordering,
+    ILU(6), 33,153 nodes (below the array's 43,690-node capacity), 26 rows a
+    level: with FP32 factors the level-synchronous sweeps split every chunk
+    over a 2-CTA cluster, so the intermediate vector in the fixed array is
+    written by two CTAs; with FP64 factors every level spans two chunks of
+    one CTA. dataflow: the same plate with the dataflow sweeps."""
+    plate = M.plate(256, 128, 1.0, 0.5, lambda x, y: 0.002 + 0 * x, "all_edges",
                     lambda q: 1e3 + 0 * q[:, 0])
     return {"single_cta": (M.plate_config2(24, 12), 2, "rcm", "level", 1),
             "split": (plate, 6, "natural", "level", 2),
@@ -55,6 +56,8 @@ def test_noalloc_apply_matches_apply_twice(precision, case):
     assert P.sweeps()["L"] == sweep
     ns = [C.c_int32(), C.c_int32()]
     assert lib.gf_precond_layout(P.h, C.byref(ns[0]), C.byref(ns[1]), None, None, None) == L.GF_OK
+    if case == "split" and precision == "fp64":
+        nsplit = 1  # two one-CTA chunks a level (see _case)
     assert (ns[0].value, ns[1].value) == (nsplit, nsplit)
     stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
     rng = np.random.default_rng(7)
