@@ -243,9 +243,9 @@ SWEEP_TRAFFIC = None
 # per row, then the converging k of smallest modelled factor + solve time) on
 # a B200. Both arms run every problem with these, so their configs match;
 # `--tune` re-runs the autotuner and prints the table it finds.
-FILLS = [12, 16, 12, 7, 6, 6, 10, 8, 12, 5, 8, 7, 10, 6, 12, 12, 10, 8, 8, 12, 12, 6, 12, 10, 6,
-         16, 12, 8, 10, 12, 12, 12, 5, 12, 5, 10, 8, 7, 5, 12, 16, 16, 8, 12, 10, 10, 10, 12, 10,
-         12, 8, 7, 16, 12, 6, 7, 8, 12, 12, 16, 4, 4, 10, 12]
+FILLS = [12, 16, 12, 7, 6, 6, 10, 8, 8, 5, 8, 6, 10, 6, 12, 12, 8, 8, 8, 12, 12, 6, 10, 10, 6,
+         16, 12, 6, 7, 8, 10, 12, 5, 12, 5, 10, 7, 6, 5, 12, 16, 16, 5, 12, 6, 10, 10, 12, 10,
+         12, 8, 7, 16, 8, 6, 5, 8, 10, 12, 16, 4, 4, 10, 12]
 ORDERS = "n" * 64  # one character per problem: "n" natural, "r" RCM
 
 
