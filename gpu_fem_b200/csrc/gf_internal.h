@@ -160,6 +160,7 @@ struct ProbDev {
   double* LU64;              // factor in ILU-pattern order (FP64)
   int nlevL, nlevU;          // triangular levels
   int32_t* done;             // per row: epoch of the factorization that finished it
+  const int32_t* pord;       // per row: slots of its lower blocks in factorization-step order
   const int32_t* levLptr;    // rows grouped by lower level (factorization order)
   const int32_t* levLrows;
   TriDesc L, U;              // chunk streams of the factor for the sweeps

@@ -29,6 +29,7 @@
 #include <cstring>
 #include <mutex>
 #include <numeric>
+#include <thread>
 #include <type_traits>
 
 #include "gf_internal.h"
@@ -280,8 +281,9 @@ constexpr int kFacPass = 6;     // passes of 5 U(k) blocks loaded at the start o
 constexpr int kFacBatch = 2;    // passes of 5 blocks in flight per lane beyond those
 constexpr int kFacMap = 1024;   // column span of a row whose column -> slot map is kept
 // per warp: values, L_ik, the diagonal block and its inverse, columns, map
+// and the row's step order
 constexpr size_t kFacWarpSmem = sizeof(double) * (36 * kFacVals + 3 * 36) +
-                                sizeof(int32_t) * kFacRow + sizeof(int16_t) * kFacMap;
+                                sizeof(int32_t) * kFacRow + sizeof(int16_t) * (kFacMap + kFacRow);
 constexpr size_t kFacSmem = kFacWarps * kFacWarpSmem;
 
 __device__ __forceinline__ int find_col(const int32_t* c, int lo, int hi, int j) {
@@ -343,6 +345,7 @@ __global__ void __launch_bounds__(kFacWarps * 32) bfactor_df(const ProbDev* __re
   double* sI = sM + 36;                        // its inverse
   int32_t* sC = reinterpret_cast<int32_t*>(sI + 36);
   int16_t* sMap = reinterpret_cast<int16_t*>(sC + kFacRow);  // column - base -> slot - r0, or -1
+  int16_t* sOrd = sMap + kFacMap;                              // step t -> slot - r0
   for (int t = lane; t < kFacMap; t += 32) sMap[t] = -1;
   __syncwarp();
   const int b = lane / 6, c = lane % 6;  // update slot and column (lanes 30, 31 idle)
@@ -367,8 +370,12 @@ __global__ void __launch_bounds__(kFacWarps * 32) bfactor_df(const ProbDev* __re
     const bool vstaged = len <= kFacVals;
     const int32_t* rc = cstaged ? sC - r0 : cols;  // rc[kp] = column of slot kp
     double* R = vstaged ? sR - 36 * (size_t)r0 : LU;  // R[36 kp + e] = entry e of slot kp
-    if (cstaged)
+    if (cstaged) {
       for (int t = lane; t < len; t += 32) sC[t] = cols[r0 + t];
+      for (int t = lane; t < di - r0; t += 32) sOrd[t] = (int16_t)(d.pord[r0 + t] - r0);
+    }
+    // slot of the row's step t (r0 <= t < di)
+    auto step_slot = [&](int t) { return cstaged ? r0 + sOrd[t - r0] : d.pord[t]; };
     // column -> slot map of the row when its column span fits (binary
     // searches otherwise)
     const int cbase = cols[r0], span = cols[r1 - 1] - cbase + 1;
@@ -395,14 +402,15 @@ __global__ void __launch_bounds__(kFacWarps * 32) bfactor_df(const ProbDev* __re
     }
     __syncwarp();
     unsigned ready = 0;  // bit s: the row of step (window start + s) is final
-    for (int kp = r0; kp < di; kp++) {
-      const int s = (kp - r0) & 31;
+    for (int st = r0; st < di; st++) {
+      const int kp = step_slot(st);
+      const int s = (st - r0) & 31;
       if (s == 0) {
         // the flags of the next 32 steps, one per lane; a lane that sees
         // its row final acquires it for the warp (the warp barrier below
         // orders that acquire before every lane's later loads)
-        const int q = kp + lane;
-        const int f = q < di ? (ld_relaxed_gpu(done + rc[q]) == epoch) : 1;
+        const int q = st + lane;
+        const int f = q < di ? (ld_relaxed_gpu(done + rc[step_slot(q)]) == epoch) : 1;
         fence_acq_rel_gpu();
         ready = __ballot_sync(0xffffffffu, f);
         __syncwarp();
@@ -1460,6 +1468,7 @@ struct gf_precond {
   DevBuf<int32_t> d_rowp, d_cols, d_diag, d_amap;
   DevBuf<int32_t> d_levLptr, d_levLrows;  // factorization order
   DevBuf<int32_t> d_done;                  // per row: epoch of the factorization that finished it
+  DevBuf<int32_t> d_ord;                   // per row: the order of its factorization steps
   long long fwork = 0;                     // block updates of one factorization
   DevBuf<double> d_lu;
   struct Tri {
@@ -1881,6 +1890,92 @@ static int sm_count() {
   return sms;
 }
 
+// Order of the factorization steps of every row (ord[r0 .. di) = slots of
+// the row's lower blocks in the order they are taken). Step k must follow
+// every step k' whose row k' has column k in its upper part (k' updates
+// A_ik), and nothing else; among the steps whose predecessors are done the
+// one whose row k has the lowest lower level goes first (ties: lower
+// column). Rows finish roughly in level order in the dataflow
+// factorization, so the steps that wait for the last-finishing rows move to
+// the end of the row and the steps after them shrink to those that really
+// depend on them. Rows longer than kOrderMax lower blocks keep ascending
+// order (complete factors: there every step depends on the previous one).
+constexpr int kOrderMax = 128;
+static void step_order_rows(const Pattern& P, const std::vector<int32_t>& diag,
+                            const std::vector<int32_t>& lv, std::vector<int32_t>& ord, int i0,
+                            int i1) {
+  std::vector<int32_t> indeg, head, nxt, to, heap;
+  for (int i = i0; i < i1; i++) {
+    const int r0 = P.rowp[i], di = diag[i], m = di - r0;
+    if (m <= 1 || m > kOrderMax) {
+      for (int t = r0; t < di; t++) ord[t] = t;
+      continue;
+    }
+    indeg.assign(m, 0);
+    head.assign(m, -1);
+    nxt.clear();
+    to.clear();
+    for (int a = 0; a < m; a++) {
+      const int k = P.cols[r0 + a];
+      // columns of U(k) that are lower columns of row i after a (both ascending)
+      int u = diag[k] + 1;
+      const int u1 = P.rowp[k + 1];
+      int b = a + 1;
+      while (u < u1 && b < m) {
+        const int cu = P.cols[u], cb = P.cols[r0 + b];
+        if (cu < cb) {
+          u++;
+        } else if (cb < cu) {
+          b++;
+        } else {
+          to.push_back(b);
+          nxt.push_back(head[a]);
+          head[a] = (int)to.size() - 1;
+          indeg[b]++;
+          u++;
+          b++;
+        }
+      }
+    }
+    // Kahn's algorithm with a min-heap on (level, column) = (lv, local index)
+    auto key = [&](int a) { return ((long long)lv[P.cols[r0 + a]] << 32) | (unsigned)a; };
+    auto cmp = [&](int x, int y) { return key(x) > key(y); };
+    heap.clear();
+    for (int a = 0; a < m; a++)
+      if (indeg[a] == 0) heap.push_back(a);
+    std::make_heap(heap.begin(), heap.end(), cmp);
+    int t = r0;
+    while (!heap.empty()) {
+      std::pop_heap(heap.begin(), heap.end(), cmp);
+      const int a = heap.back();
+      heap.pop_back();
+      ord[t++] = r0 + a;
+      for (int e = head[a]; e >= 0; e = nxt[e])
+        if (--indeg[to[e]] == 0) {
+          heap.push_back(to[e]);
+          std::push_heap(heap.begin(), heap.end(), cmp);
+        }
+    }
+  }
+}
+// Rows are independent: host threads take contiguous row ranges.
+static void step_order(const Pattern& P, const std::vector<int32_t>& diag,
+                       const std::vector<int32_t>& lv, std::vector<int32_t>& ord) {
+  const int n = P.n;
+  ord.assign(P.nnz(), 0);
+  const int nt = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  if (nt == 1 || n < 4096) {
+    step_order_rows(P, diag, lv, ord, 0, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  for (int t = 0; t < nt; t++) {
+    const int i0 = (int)((long long)n * t / nt), i1 = (int)((long long)n * (t + 1) / nt);
+    th.emplace_back([&, i0, i1] { step_order_rows(P, diag, lv, ord, i0, i1); });
+  }
+  for (auto& x : th) x.join();
+}
+
 // CTAs of the dataflow factorization for one problem given `budget` CTAs for
 // it: at least one, at most one per 32 rows (four rows per warp) and 128.
 static int fac_ctas_cap(const gf_precond* p, int budget) {
@@ -1937,6 +2032,7 @@ static gf_status upload_desc(gf_batch* B) {
     d.LU64 = p->d_lu.p;
     d.nlevL = p->nlevL;
     d.done = p->d_done.p;
+    d.pord = p->d_ord.p;
     d.nlevU = p->nlevU;
     d.levLptr = p->d_levLptr.p;
     d.levLrows = p->d_levLrows.p;
@@ -2602,6 +2698,11 @@ gf_status gf_precond_create_ex(gf_assembler* a, int32_t fill_level, int32_t prec
   up(p->d_levLrows.upload(lrows));
   up(p->d_lu.alloc((size_t)36 * p->pat.nnz()));
   up(p->d_done.alloc((size_t)n));
+  {
+    std::vector<int32_t> ord;
+    step_order(p->pat, diag, p->lvL, ord);
+    up(p->d_ord.upload(ord));
+  }
   if (e == cudaSuccess) up(cudaMemset(p->d_done.p, 0, sizeof(int32_t) * (size_t)n));
   // block updates of one factorization: per step (i, k) the block L_ik and
   // one update per block of U(k)
