@@ -234,9 +234,13 @@ def _dist():
     return ws, rank, local
 
 
-# DRAM bytes (read + write) of one launch of the sweep kernel on this
-# workload, from an ncu capture (profiles/); None until measured.
-SWEEP_TRAFFIC = None
+# DRAM bytes (read + write) of a sweep launch over its algorithmic bytes,
+# from an ncu capture of the 256x128 ILU(6) FP32 sweep case (the batch's
+# launches are too large to capture): 85.1 MB / 80.2 MB for L, 89.7 MB /
+# 85.1 MB for U (profiles/bsweep_tma_256x128_ilu6_traffic.md). Traffic per
+# launch grows with the blocks streamed, so the bench scales the ratio by its
+# own algorithmic bytes per launch.
+SWEEP_TRAFFIC_RATIO = 1.055
 
 # Fill level k and node ordering of each of the 64 problems, as chosen by the
 # batch autotuner (gpu_fem_b200/batch.py: ordering by ILU(8) levels x blocks
@@ -557,7 +561,11 @@ def main():
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d},
         "roofline": {"kernel": "bsweep_tma (block L and U sweeps, FP32 factor values)",
                      "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": SWEEP_TRAFFIC,
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": SWEEP_TRAFFIC_RATIO * sweep_bytes / max(sweep_launches, 1),
+                     "traffic_note": "DRAM read+write per launch: ncu ratio traffic/algorithmic "
+                                     "bytes of the 256x128 ILU(6) sweep case x this run's "
+                                     "algorithmic bytes per launch",
                      "launches": sweep_launches,
                      "ms_per_launch": sweep_ms / max(sweep_launches, 1),
                      "algorithmic_bytes_per_launch": sweep_bytes / max(sweep_launches, 1),

@@ -87,21 +87,20 @@ ORDERINGS = ("natural", "rcm")
 def factor_cost_us(nrow, inf):
     """One numeric factorization of a problem (microseconds), fitted to B200
     runs of single plates (16^2 to 256^2 elements, fills 1 to 16) on the
-    dataflow factorization. RCM-ordered factors cost ~7.6 us a lower level:
-    a row waits for its last-finishing dependency and then has only a few
-    steps left. In natural order the rows along a grid line depend on their
-    neighbour and run their same-line steps after the previous line's rows,
-    so a level costs more as rows get longer, and the block updates
+    dataflow factorization with dependency-ordered steps: ~7-9 us a lower
+    level (a row waits for its last-finishing dependency, then has only the
+    steps that depend on it left), a little more per level as rows get
+    longer, and a small throughput term for the block updates
     (~nrow x lower x (lower + 1), lower = blocks left of the diagonal per
-    row) spread over the warps add a throughput term."""
+    row) spread over the warps."""
     lvl, nnzb = inf["levels_L"], inf["nnzb"]
     lower = max(nnzb - nrow, 0) / (2.0 * nrow)
     warps = 8 * max(1, min(128, nrow // 32))
     work = nrow * lower * (lower + 1.0)
     if inf.get("ordering", "natural") == "rcm":
-        t = 7.65 * lvl + 0.0049 * lvl * lower + 0.003 * lvl * lower * lower - 0.076 * work / warps - 72.0
+        t = 7.19 * lvl - 0.0132 * lvl * lower + 0.0031 * lvl * lower * lower + 0.028 * work / warps - 2.9
     else:
-        t = 12.09 * lvl - 0.572 * lvl * lower + 0.0099 * lvl * lower * lower + 1.68 * work / warps - 394.5
+        t = 8.56 * lvl - 0.101 * lvl * lower + 0.0040 * lvl * lower * lower + 0.143 * work / warps - 40.9
     return max(t, 20.0)
 
 
