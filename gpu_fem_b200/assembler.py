@@ -401,3 +401,19 @@ def gmres_solve(assembler, mat, precond, b: torch.Tensor, x: torch.Tensor, opts=
     return st, {"iterations": stats.iterations, "restarts": stats.restarts,
                 "refinements": stats.refinements, "status": stats.status,
                 "rel_residual": stats.rel_residual, "time_ms": stats.time_ms}
+
+
+def direct_solve(assembler, mat, b: torch.Tensor, x: torch.Tensor, raise_on_fail=True):
+    """Complete block LU solve of CUSPARSE::direct_LU_solve_old
+    (include/linalg/solvers/cusparse.h:16-192) through gf_direct_solve: the
+    full-fill factor on the ILU kernels, applied with GMRES refinement to the
+    FP64 residual floor."""
+    stats = L.gf_solve_stats()
+    st = L.lib().gf_direct_solve(assembler.h, mat.h, _ptr(b), _ptr(x), C.byref(stats), _stream())
+    if raise_on_fail:
+        check(st, "direct_solve")
+    return st, {"iterations": stats.iterations, "status": stats.status,
+                "rel_residual": stats.rel_residual, "time_ms": stats.time_ms}
+
+
+direct_LU_solve_old = direct_solve
