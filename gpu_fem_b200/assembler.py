@@ -366,6 +366,14 @@ class ILUk_Preconditioner:
         return {"nsplit_L": v[0].value, "nsplit_U": v[1].value, "fac_ctas": v[2].value,
                 "chunks_L": v[3].value, "chunks_U": v[4].value}
 
+    def setup_info(self):
+        """gf_precond_setup_info: whether the ILU(k) pattern was computed on
+        the GPU, and the host wall times (ms) of the pattern and the setup."""
+        g, sm, tm = C.c_int32(), C.c_double(), C.c_double()
+        check(L.lib().gf_precond_setup_info(self.h, C.byref(g), C.byref(sm), C.byref(tm)),
+              "setup_info")
+        return {"symbolic_on_gpu": bool(g.value), "symbolic_ms": sm.value, "setup_ms": tm.value}
+
     def status(self):
         """gf_precond_status: reads and clears the device-side status flags."""
         return L.lib().gf_precond_status(self.h, _stream())

@@ -89,6 +89,10 @@ void elem_ind_map(int nelem, const int32_t* conn, const Pattern& p,
                   const std::vector<int32_t>& perm, std::vector<int32_t>& map);
 // computeILUk (include/linalg/bsr_utils.h:678-807).
 Pattern iluk_pattern(const Pattern& a, int lev);
+// The same pattern computed on the GPU (symbolic_gpu.cu); false when a row's
+// column window exceeds the kernel's or the device fails, and the caller
+// then uses iluk_pattern.
+bool iluk_pattern_gpu(const Pattern& a, int lev, Pattern& out);
 // Level sets of the lower / upper triangular DAG.
 int levels(const Pattern& p, bool lower, std::vector<int32_t>& level);
 

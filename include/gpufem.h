@@ -281,6 +281,14 @@ gf_status gf_precond_status(gf_precond* p, void* stream);
  * level with more blocks than a chunk's stage spans several). Any pointer
  * may be NULL. No reference counterpart (cuSPARSE's bsrsv2 level analysis is
  * internal). */
+/* Where and how long the preconditioner's setup ran: whether its ILU(k)
+ * pattern was computed on the GPU (1; 0 when the host computed it: fill 0,
+ * a row whose column window exceeds the GPU kernel's 4096, or a device
+ * failure), the wall time of that pattern and of the whole
+ * gf_precond_create (ms). Any pointer may be NULL. No reference counterpart
+ * (computeILUk, include/linalg/bsr_utils.h:678-807, runs on the host). */
+gf_status gf_precond_setup_info(const gf_precond* p, int32_t* symbolic_on_gpu, double* symbolic_ms,
+                                double* setup_ms);
 gf_status gf_precond_layout(const gf_precond* p, int32_t* nsplit_L, int32_t* nsplit_U,
                             int32_t* fac_ctas, int32_t* chunks_L, int32_t* chunks_U);
 /* Pattern, level count and factor copy for checking. rowPtr/colPtr may be
