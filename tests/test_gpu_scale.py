@@ -9,18 +9,17 @@ with right-preconditioned GMRES on the GPU, once with FP64 factors and once
 with FP32 factors inside FP64 GMRES (the mixed mode), and the displacement
 error against the golden is checked and printed per solve.
 
-Gate: ||x - x_golden|| / ||x_golden|| <= max(1e-8, 3 * (fp64_noise + k_noise)).
+Gate: ||x - x_golden|| / ||x_golden|| <= max(1e-8, 3 * max(fp64_noise, k_noise)).
 Both noise figures are computed with each golden: fp64_noise is how far an
 exactly factored FP64 solve still moves under refinement with FP64
 residuals, and k_noise is how far x moves when every entry of K is perturbed
 by one rounding (a relative eps), i.e. how precisely any FP64 assembly of K
-defines x. A GPU solve carries both at once (its own K rounding and a stop
-at the residual floor), so the two add. For the plates of the batch workload and for the box both are far
+defines x. For the plates of the batch workload and for the box both are far
 below 1e-8 (box: 4.7e-12 and 8.2e-12) and the gate is 1e-8. The jittered
 cantilever (2 x 1 m, t = 4 mm, one edge clamped) is the exception: one
 rounding of K moves its x by 1.0e-8 at 100 x 50 and by 8.2e-8 at its stated
 400 x 200, so two correct FP64 assemblies and solves can differ by that much
-and the gate there is 4.2e-8 and 3.0e-7. Its relative residual cannot go
+and the gate there is 3.1e-8 and 2.5e-7. Its relative residual cannot go
 below eps || |K| |x| || / ||b|| (3.0e-7 and 4.8e-6: the residual of x rounded
 to FP64) for any solver, so its GMRES tolerance is that floor; the
 workload's 1e-8 residual is out of reach for it in FP64. At 400 x 200 block
@@ -64,7 +63,7 @@ def _solve(mesh, ordering, fill, precision, rtol, restart=100, max_iters=20000):
 def _check(name, x, g, stats, label):
     idx = g["idx"]
     err = np.linalg.norm(x[idx] - g["x"]) / np.linalg.norm(g["x"])
-    bound = max(1e-8, 3.0 * (float(g["fp64_noise"]) + float(g["k_noise"])))
+    bound = max(1e-8, 3.0 * max(float(g["fp64_noise"]), float(g["k_noise"])))
     print(f"{name} {label}: rel residual {stats['rel_residual']:.2e}, "
           f"{stats['iterations']} GMRES steps, displacement error {err:.2e} (gate {bound:.2e})")
     assert err <= bound, (name, label, err, bound, stats)
