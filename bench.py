@@ -66,7 +66,7 @@ def _args():
     return ap.parse_args()
 
 
-SERVE_RATE, SERVE_MAX_CLASS = 10.0, 4
+SERVE_RATE, SERVE_MAX_CLASS = 20.0, 4
 
 
 def serving_run(seconds):
@@ -103,11 +103,15 @@ def serving_run(seconds):
 
 def assembly_case():
     """Jacobian assembly with fused BCs of the 400x200 plate (80,601 nodes,
-    ~209 MB of block values, above L2), 5 times: the small case on which the
-    assembly kernel is profiled."""
+    ~209 MB of block values, above L2), 5 times with the coloured scatter:
+    the small case on which the assembly kernel is profiled. Then prints the
+    event-timed Jacobian with the coloured and the atomic scatter, alone and
+    for the 64-plate batch (one launch per colour over all problems, or one
+    launch with atomics)."""
     import torch
     from gpu_fem_b200 import mesh as M
-    from gpu_fem_b200.assembler import ElementAssembler, createBsrMat
+    from gpu_fem_b200.assembler import ElementAssembler, ILUk_Preconditioner, createBsrMat
+    from gpu_fem_b200.batch import Batch
     m = M.plate_config2()
     A = ElementAssembler.from_mesh(m, ordering="rcm")
     K = createBsrMat(A)
@@ -116,6 +120,28 @@ def assembly_case():
         A.add_jacobian(res, K, fuse_bcs=True)
     torch.cuda.synchronize()
     print("assembly case", A.get_nnzb())
+
+    def timed(fn, reps=10):
+        fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    out = {"400x200 coloured ms": timed(lambda: A.add_jacobian(None, K, fuse_bcs=True)),
+           "400x200 atomic ms": timed(lambda: A.add_jacobian(None, K, fuse_bcs=True, atomic=True))}
+    meshes = M.batch_config4(64)
+    asms = [ElementAssembler.from_mesh(mm, ordering="natural") for mm in meshes]
+    mats = [createBsrMat(a) for a in asms]
+    pcs = [ILUk_Preconditioner(a, fill_level=0) for a in asms]
+    bt = Batch(asms, mats, pcs)
+    out["batch64 coloured ms"] = timed(bt.assemble)
+    bt.set_scatter(True)
+    out["batch64 atomic ms"] = timed(bt.assemble)
+    print("assembly scatter", json.dumps({k: round(v, 3) for k, v in out.items()}))
 
 
 def sweep_case(kind):

@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(_HERE, "libgpufem.so")
 GF_OK, GF_INVALID_ARG, GF_OOM, GF_ZERO_PIVOT, GF_NOT_CONVERGED, GF_NAN, GF_TIMEOUT, \
     GF_CUDA_ERROR, GF_NO_DEVICE, GF_OVER_BUDGET = range(10)
 GF_ORDER_NATURAL, GF_ORDER_RCM, GF_ORDER_QORDER = 0, 1, 2
-GF_ASSEMBLE_OVERWRITE, GF_ASSEMBLE_ADD, GF_ASSEMBLE_FUSE_BCS = 0, 1, 2
+GF_ASSEMBLE_OVERWRITE, GF_ASSEMBLE_ADD, GF_ASSEMBLE_FUSE_BCS, GF_ASSEMBLE_ATOMIC = 0, 1, 2, 4
 GF_PREC_FP64, GF_PREC_FP32 = 0, 1
 GF_SWEEP_AUTO, GF_SWEEP_DATAFLOW, GF_SWEEP_LEVEL = 0, 1, 2
 GF_FILL_FULL = 0x7FFFFFFF
@@ -111,6 +111,7 @@ SIGNATURES = {
     "gf_precond_info": (_I, [_P, _PI, _PI, _PI]),
     "gf_precond_status": (_I, [_P, _P]),
     "gf_precond_layout": (_I, [_P, _PI, _PI, _PI, _PI, _PI]),
+    "gf_batch_set_scatter": (_I, [_P, C.c_int32]),
     "gf_precond_setup_info": (_I, [_P, _PI, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "gf_test_set_waits": (_I, [C.c_ulonglong, _I]),
     "gf_precond_get": (_I, [_P, _PI, _PI, _PD]),

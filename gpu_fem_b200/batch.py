@@ -59,6 +59,12 @@ class Batch:
     def assemble(self):
         L.check(L.lib().gf_batch_assemble(self.h, _stream()), "gf_batch_assemble")
 
+    def set_scatter(self, atomic):
+        """Batched assembly scatter: coloured (bitwise reproducible, one launch
+        per colour over all problems) or FP64 atomics (one launch)."""
+        L.check(L.lib().gf_batch_set_scatter(self.h, L.GF_ASSEMBLE_ATOMIC if atomic else 0),
+                "gf_batch_set_scatter")
+
     def factor(self):
         L.check(L.lib().gf_batch_factor(self.h, _stream()), "gf_batch_factor")
 

@@ -18,8 +18,16 @@
 //     one colour share no node and run concurrently (one launch per colour);
 //     inside a chunk the warp handles its elements in order. The first
 //     toucher of a block stores, later touchers read-modify-write; there are
-//     no atomics and the result is bitwise reproducible.
+//     no atomics and the result is bitwise reproducible;
+//   * with GF_ASSEMBLE_ATOMIC the colours are ignored: the outputs are zeroed
+//     and one launch over all chunks adds with FP64 atomics (the reference's
+//     scatter; sums in arrival order, so not bitwise reproducible);
+//   * a batch of problems runs each colour of all its problems in one launch
+//     (work items = (problem, chunk) per warp), or all chunks of all
+//     problems in one launch with atomics.
+#include <algorithm>
 #include <cstdio>
+#include <cstring>
 
 #include "gf_internal.h"
 
@@ -165,7 +173,10 @@ __device__ void process_element(int s, int k, WarpSlot& w, const AsmParams& P, i
           v[6 * r + c] = x;
         }
       double2* d2 = reinterpret_cast<double2*>(dst);
-      if (first && !add) {
+      if (P.flags & GF_ASSEMBLE_ATOMIC) {
+#pragma unroll
+        for (int h = 0; h < 18; h++) atomicAdd(dst + h, v[h]);
+      } else if (first && !add) {
 #pragma unroll
         for (int h = 0; h < 9; h++) d2[h] = make_double2(v[2 * h], v[2 * h + 1]);
       } else {
@@ -188,7 +199,9 @@ __device__ void process_element(int s, int k, WarpSlot& w, const AsmParams& P, i
       if (fuse && ((P.bcmask[nodes[a]] >> r) & 1)) val = 0.0;
       double* dst = P.res + 6 * (size_t)nodes[a] + r;
       const bool first = (ft >> (16 + a)) & 1;
-      if (first && !add)
+      if (P.flags & GF_ASSEMBLE_ATOMIC)
+        atomicAdd(dst, val);
+      else if (first && !add)
         *dst = val;
       else
         *dst += val;
@@ -222,7 +235,9 @@ __device__ void process_element(int s, int k, WarpSlot& w, const AsmParams& P, i
         if (fuse && ((P.bcmask[nodes[b]] >> c) & 1)) rj = 0.0;
         double* dst = P.res + 6 * (size_t)nodes[b] + c;
         const bool first = (ft >> (16 + b)) & 1;
-        if (first && !add)
+        if (P.flags & GF_ASSEMBLE_ATOMIC)
+          atomicAdd(dst, rj);
+        else if (first && !add)
           *dst = rj;
         else
           *dst += rj;
@@ -246,6 +261,29 @@ __global__ void __launch_bounds__(kAsmWarps * 32)
   batch_geometry(s0, cnt, w, P, lane);
   for (int k = 0; k < cnt; k++) process_element<MODE>(s0 + k, k, w, P, lane, energy_acc);
   if (MODE == MODE_ENERGY && lane == 0) P.energy_part[li] = energy_acc;
+}
+
+// Batched form: warp w of the launch works on chunk work[w].y of problem
+// work[w].x, whose parameters are copied to shared memory first.
+template <int MODE>
+__global__ void __launch_bounds__(kAsmWarps * 32)
+    assemble_batch_kernel(const AsmParams* __restrict__ PP, const int2* __restrict__ work,
+                          int nwork) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  WarpSlot* slots = reinterpret_cast<WarpSlot*>(smem_raw);
+  __shared__ AsmParams sp[kAsmWarps];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int wi = blockIdx.x * kAsmWarps + warp;
+  if (wi >= nwork) return;
+  const int2 it = work[wi];
+  if (lane == 0) sp[warp] = PP[it.x];
+  __syncwarp();
+  const AsmParams& P = sp[warp];
+  const int s0 = P.chunk_start[it.y], cnt = P.chunk_start[it.y + 1] - s0;
+  WarpSlot& w = slots[warp];
+  double energy_acc = 0.0;
+  batch_geometry(s0, cnt, w, P, lane);
+  for (int k = 0; k < cnt; k++) process_element<MODE>(s0 + k, k, w, P, lane, energy_acc);
 }
 
 __global__ void sum_kernel(const double* part, int n, double* out) {
@@ -325,6 +363,20 @@ static gf_status launch_assembly(gf_assembler* a, double* values, double* res, i
   GF_CUDA(cudaFuncSetAttribute(assemble_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)smem));
   const Schedule& s = a->sched;
+  if (flags & GF_ASSEMBLE_ATOMIC) {
+    if (!(flags & GF_ASSEMBLE_ADD)) {
+      if (values) GF_CUDA(cudaMemsetAsync(values, 0, sizeof(double) * 36 * (size_t)a->pat.nnz(), st));
+      if (res) GF_CUDA(cudaMemsetAsync(res, 0, sizeof(double) * 6 * (size_t)a->nnodes, st));
+    }
+    P.chunk_base = 0;
+    P.chunk_end = s.nchunks;
+    const int nblk = (s.nchunks + kAsmWarps - 1) / kAsmWarps;
+    if (nblk > 0) {
+      assemble_kernel<MODE><<<nblk, kAsmWarps * 32, smem, st>>>(P); ::gf::count_launch();
+      GF_CHECK_LAUNCH();
+    }
+    return GF_OK;
+  }
   for (int cc = 0; cc < s.ncc; cc++) {
     const int nch = s.cc_start[cc + 1] - s.cc_start[cc];
     if (nch == 0) continue;
@@ -332,6 +384,95 @@ static gf_status launch_assembly(gf_assembler* a, double* values, double* res, i
     P.chunk_base = s.cc_start[cc];
     P.chunk_end = s.cc_start[cc + 1];
     assemble_kernel<MODE><<<nblk, kAsmWarps * 32, smem, st>>>(P); ::gf::count_launch();
+    GF_CHECK_LAUNCH();
+  }
+  return GF_OK;
+}
+
+// Cached launch data of a batch's assembly: per-problem parameters (rebuilt
+// when a problem's thickness pointer or the flags change) and the work lists.
+struct BatchAsm {
+  std::vector<AsmParams> host;
+  DevBuf<AsmParams> d_params;
+  DevBuf<int2> d_work;
+  std::vector<int> off;  // work ranges: per colour (coloured) or one (atomic)
+  int flags = -1;
+};
+
+void batch_asm_free(BatchAsm* b) { delete b; }
+
+gf_status batch_assemble(BatchAsm*& cache, const std::vector<gf_assembler*>& asms,
+                         const std::vector<double*>& values, const double* const* thick,
+                         int flags, cudaStream_t st) {
+  const int np = (int)asms.size();
+  if (!cache) cache = new BatchAsm();
+  BatchAsm& B = *cache;
+  std::vector<AsmParams> h(np);
+  for (int k = 0; k < np; k++) {
+    gf_assembler* a = asms[k];
+    AsmParams& P = h[k];
+    std::memset(&P, 0, sizeof(P));
+    P.xpts = a->d_xpts.p;
+    P.vars = a->d_vars.p;
+    P.bcmask = a->d_bcmask.p;
+    P.sconn = a->d_sconn.p;
+    P.semap = a->d_semap.p;
+    P.sft = a->d_sft.p;
+    P.sthick = a->d_sthick.p;
+    P.smat = a->d_smat.p;
+    P.mats = a->d_mats.p;
+    P.chunk_start = a->d_chunk_start.p;
+    P.thick_nat = thick ? thick[k] : nullptr;
+    P.sorder = a->d_sorder.p;
+    P.values = values[k];
+    P.res = nullptr;
+    P.energy_part = a->d_energy_part.p;
+    P.flags = flags;
+  }
+  const bool atomic = (flags & GF_ASSEMBLE_ATOMIC) != 0;
+  if (B.flags != flags || B.host.size() != h.size() ||
+      std::memcmp(B.host.data(), h.data(), sizeof(AsmParams) * h.size()) != 0) {
+    // work items: (problem, chunk), colour by colour, or all chunks at once
+    std::vector<int2> work;
+    B.off.assign(1, 0);
+    if (atomic) {
+      for (int k = 0; k < np; k++)
+        for (int c = 0; c < asms[k]->sched.nchunks; c++) work.push_back(make_int2(k, c));
+      B.off.push_back((int)work.size());
+    } else {
+      int ncc = 0;
+      for (auto* a : asms) ncc = std::max(ncc, a->sched.ncc);
+      for (int cc = 0; cc < ncc; cc++) {
+        for (int k = 0; k < np; k++) {
+          const Schedule& s = asms[k]->sched;
+          if (cc >= s.ncc) continue;
+          for (int c = s.cc_start[cc]; c < s.cc_start[cc + 1]; c++) work.push_back(make_int2(k, c));
+        }
+        B.off.push_back((int)work.size());
+      }
+    }
+    GF_CUDA(B.d_work.alloc(work.size()));
+    GF_CUDA(B.d_params.alloc(h.size()));
+    GF_CUDA(cudaMemcpyAsync(B.d_work.p, work.data(), sizeof(int2) * work.size(),
+                            cudaMemcpyHostToDevice, st));
+    GF_CUDA(cudaMemcpyAsync(B.d_params.p, h.data(), sizeof(AsmParams) * h.size(),
+                            cudaMemcpyHostToDevice, st));
+    GF_CUDA(cudaStreamSynchronize(st));  // the host copies are reused
+    B.host = h;
+    B.flags = flags;
+  }
+  if (atomic && !(flags & GF_ASSEMBLE_ADD))
+    for (int k = 0; k < np; k++)
+      GF_CUDA(cudaMemsetAsync(values[k], 0, sizeof(double) * 36 * (size_t)asms[k]->pat.nnz(), st));
+  const size_t smem = sizeof(WarpSlot) * kAsmWarps;
+  GF_CUDA(cudaFuncSetAttribute(assemble_batch_kernel<MODE_JAC>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  for (size_t r = 0; r + 1 < B.off.size(); r++) {
+    const int nwork = B.off[r + 1] - B.off[r];
+    if (nwork == 0) continue;
+    assemble_batch_kernel<MODE_JAC><<<(nwork + kAsmWarps - 1) / kAsmWarps, kAsmWarps * 32, smem,
+                                      st>>>(B.d_params.p, B.d_work.p + B.off[r], nwork);
+    ::gf::count_launch();
     GF_CHECK_LAUNCH();
   }
   return GF_OK;

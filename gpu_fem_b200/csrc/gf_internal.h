@@ -169,6 +169,11 @@ struct ProbDev {
   const int32_t* levLrows;
   TriDesc L, U;              // chunk streams of the factor for the sweeps
 };
+// Batched Jacobian assembly with fused BCs (assembly.cu): one launch per
+// colour over all problems, or one launch with GF_ASSEMBLE_ATOMIC; `cache`
+// holds the launch data between calls (batch_asm_free releases it).
+struct BatchAsm;
+void batch_asm_free(BatchAsm* b);
 int build_schedule(int nelem, int nnodes, const int32_t* conn, const std::vector<int32_t>& emap,
                    int nnzb, int chunk_size, Schedule& s);
 
@@ -211,3 +216,9 @@ struct gf_bsr {
   gf::DevBuf<gf::ProbDev> desc;       // one-entry table for gf_bsr_spmv
   gf::DevBuf<int32_t> rowprob;
 };
+
+namespace gf {
+gf_status batch_assemble(BatchAsm*& cache, const std::vector<gf_assembler*>& asms,
+                         const std::vector<double*>& values, const double* const* thick, int flags,
+                         cudaStream_t st);
+}  // namespace gf

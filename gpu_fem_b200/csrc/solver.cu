@@ -1880,7 +1880,10 @@ struct gf_batch {
   DevBuf<double> V, H, g, cs, ss, y, h, hn, target, partial, pnorm, w, t, r, d, e, norms, bnorm;
   DevBuf<double> tfac;
   DevBuf<int> jcnt, run, live, live2;
+  gf::BatchAsm* basm = nullptr;  // launch data of the batched assembly
+  int scatter = 0;               // 0: coloured, GF_ASSEMBLE_ATOMIC: atomic
   Chunks chunks() const { return Chunks{nchunks, d_cprob.p, d_clo.p, d_chi.p, d_pstart.p}; }
+  ~gf_batch() { gf::batch_asm_free(basm); }
 };
 
 namespace gf {
@@ -2986,24 +2989,20 @@ gf_status gf_batch_destroy(gf_batch* b) {
 }
 
 gf_status gf_batch_assemble(gf_batch* B, void* stream) {
-  if (!B) return GF_INVALID_ARG;
-  for (int k = 0; k < B->np; k++) {
-    gf_status s = gf_add_jacobian(B->asms[k], nullptr, B->mats[k], GF_ASSEMBLE_FUSE_BCS, stream);
-    if (s != GF_OK) return s;
-  }
-  return GF_OK;
+  return gf_batch_assemble_ex(B, nullptr, stream);
 }
 
 gf_status gf_batch_assemble_ex(gf_batch* B, const double* const* d_thick, void* stream) {
   if (!B) return GF_INVALID_ARG;
-  for (int k = 0; k < B->np; k++) {
-    gf_status s = (d_thick && d_thick[k])
-                      ? gf_add_jacobian_thick(B->asms[k], d_thick[k], nullptr, B->mats[k],
-                                              GF_ASSEMBLE_FUSE_BCS, stream)
-                      : gf_add_jacobian(B->asms[k], nullptr, B->mats[k], GF_ASSEMBLE_FUSE_BCS,
-                                        stream);
-    if (s != GF_OK) return s;
-  }
+  std::vector<double*> values(B->np);
+  for (int k = 0; k < B->np; k++) values[k] = B->mats[k]->vals.p;
+  return batch_assemble(B->basm, B->asms, values, d_thick, GF_ASSEMBLE_FUSE_BCS | B->scatter,
+                        as_stream(stream));
+}
+
+gf_status gf_batch_set_scatter(gf_batch* B, int32_t flags) {
+  if (!B || (flags != 0 && flags != GF_ASSEMBLE_ATOMIC)) return GF_INVALID_ARG;
+  B->scatter = flags;
   return GF_OK;
 }
 

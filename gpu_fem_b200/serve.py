@@ -120,6 +120,30 @@ class Group:
                            [s["P"] for s in self.slots])
         n = size
         self.thick_ptrs = (C.c_void_p * n)(*[s["thick"].data_ptr() for s in self.slots])
+        self.atomic = self.tune_scatter()
+
+    def tune_scatter(self, reps=3):
+        """Times this group's assembly with the coloured scatter (one launch
+        per colour) and the atomic one (one launch, FP64 atomics) and keeps
+        the faster: atomics pay where the colours' launches dominate."""
+        def timed():
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            L.check(L.lib().gf_batch_assemble_ex(self.batch.h, self.thick_ptrs, _stream()),
+                    "assemble")
+            e0.record()
+            for _ in range(reps):
+                L.check(L.lib().gf_batch_assemble_ex(self.batch.h, self.thick_ptrs, _stream()),
+                        "assemble")
+            e1.record()
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1)
+        self.batch.set_scatter(False)
+        t_col = timed()
+        self.batch.set_scatter(True)
+        t_atom = timed()
+        atomic = t_atom < t_col
+        self.batch.set_scatter(atomic)
+        return atomic
 
     def run(self, reqs, server):
         """Assemble, factor and solve the group with `reqs` in its first slots."""

@@ -79,7 +79,17 @@ typedef struct gf_mesh_desc {
  * qorder_seed; the reference seeds from std::random_device. */
 enum { GF_ORDER_NATURAL = 0, GF_ORDER_RCM = 1, GF_ORDER_QORDER = 2 };
 
-enum { GF_ASSEMBLE_OVERWRITE = 0, GF_ASSEMBLE_ADD = 1, GF_ASSEMBLE_FUSE_BCS = 2 };
+/* GF_ASSEMBLE_ATOMIC: scatter with FP64 atomics in one launch over all
+ * element chunks (the reference's scatter, include/linalg/bsr_mat.h:229-276)
+ * instead of the coloured, bitwise-reproducible schedule (one launch per
+ * colour); the outputs are zeroed first unless GF_ASSEMBLE_ADD is set, and
+ * sums are taken in arrival order. */
+enum {
+  GF_ASSEMBLE_OVERWRITE = 0,
+  GF_ASSEMBLE_ADD = 1,
+  GF_ASSEMBLE_FUSE_BCS = 2,
+  GF_ASSEMBLE_ATOMIC = 4
+};
 
 typedef struct gf_assembler gf_assembler;
 typedef struct gf_bsr gf_bsr;
@@ -372,6 +382,11 @@ gf_status gf_batch_assemble(gf_batch* b, void* stream);
  * NULL to use the assembler's own). */
 gf_status gf_batch_assemble_ex(gf_batch* b, const double* const* d_thick, void* stream);
 /* Numeric ILU(k) of every problem in one level-ordered launch. */
+/* Scatter of the batch's assembly (gf_batch_assemble / _ex): 0 (default)
+ * runs each colour of all problems in one launch (coloured, bitwise
+ * reproducible), GF_ASSEMBLE_ATOMIC runs all chunks of all problems in one
+ * launch with FP64 atomics. No reference counterpart. */
+gf_status gf_batch_set_scatter(gf_batch* b, int32_t flags);
 gf_status gf_batch_factor(gf_batch* b, void* stream);
 /* Solve every problem: d_b[k], d_x[k] device pointers (natural order,
  * d_x[k] is the initial guess); stats[k] per problem (may be NULL). */
