@@ -113,14 +113,19 @@ class Group:
     a dispatch fills up to len(slots) requests into it; slots it leaves empty
     get a zero load and drop out of the solve at its first residual check."""
 
-    def __init__(self, cls, size):
+    def __init__(self, cls, size, scatter="tune"):
         self.cls = cls
         self.slots = [cls.make_slot() for _ in range(size)]
         self.batch = Batch([cls.asm] * size, [s["K"] for s in self.slots],
                            [s["P"] for s in self.slots])
         n = size
         self.thick_ptrs = (C.c_void_p * n)(*[s["thick"].data_ptr() for s in self.slots])
-        self.atomic = self.tune_scatter()
+        # assembly scatter: timed per group ("tune"), or fixed
+        if scatter == "tune":
+            self.atomic = self.tune_scatter()
+        else:
+            self.atomic = scatter == "atomic"
+            self.batch.set_scatter(self.atomic)
 
     def tune_scatter(self, reps=3):
         """Times this group's assembly with the coloured scatter (one launch
@@ -218,7 +223,7 @@ class SizeClass:
         for size in sorted(sizes, reverse=True):
             torch.cuda.synchronize()
             before = torch.cuda.mem_get_info()[0]
-            g = Group(self, size)
+            g = Group(self, size, server.scatter)
             g.run([], server)
             used = before - torch.cuda.mem_get_info()[0]
             if self.groups and self.reserved_bytes + used > budget_bytes:
@@ -269,8 +274,12 @@ class Server:
     GROUP_SIZES = (8, 4, 2, 1)
 
     def __init__(self, budget_gb=120.0, streams=4, max_batch=8, classes=None, restart=100,
-                 rtol=1e-8, fills=None, max_iters=3000, precision="fp32"):
+                 rtol=1e-8, fills=None, max_iters=3000, precision="fp32", scatter="tune"):
         self.budget = budget_gb * 1e9
+        # assembly scatter of the slot groups: "tune" (each group times the
+        # coloured and the atomic scatter and keeps the faster), "coloured"
+        # (bitwise reproducible) or "atomic"
+        self.scatter = scatter
         self.max_batch = max_batch
         self.restart, self.rtol, self.max_iters = restart, rtol, max_iters
         self.precision = precision  # ILU factor values: "fp32" (mixed) or "fp64"
@@ -337,7 +346,7 @@ class Server:
     def solve_alone(self, req):
         """Solve one request by itself (a group of one built for it) and return x."""
         cls = self.get_class(req.family, req.cls)
-        g = Group(cls, 1)
+        g = Group(cls, 1, self.scatter)
         g.run([req], self)
         torch.cuda.synchronize()
         return g.slots[0]["x"].cpu().numpy().copy()

@@ -1,6 +1,7 @@
 """Continuous-batching server: a short Poisson stream of plate and box
-requests over the smallest size classes is served to 1e-8; a request's
-displacement is the same served in the mix as solved alone."""
+requests over the smallest size classes is served to 1e-8; with the coloured
+(bitwise-reproducible) assembly scatter a request's displacement is bitwise
+the same served in the mix as solved alone."""
 import numpy as np
 import pytest
 
@@ -11,7 +12,7 @@ def test_server_stream_and_alone_equals_mix():
     from gpu_fem_b200 import serve
     reqs = serve.poisson_requests(rate=30.0, duration=1.0, seed=99, max_class=2)
     assert len(reqs) >= 10
-    srv = serve.Server(budget_gb=8.0, streams=2, max_batch=8)
+    srv = serve.Server(budget_gb=8.0, streams=2, max_batch=8, scatter="coloured")
     srv.warm({(r.family, r.cls) for r in reqs})
     srv.keep_results = True
     out = srv.run(reqs)
