@@ -71,7 +71,7 @@ SERVE_RATE, SERVE_MAX_CLASS = 20.0, 4
 
 def serving_run(seconds):
     """Continuous-batching server on a Poisson stream of plate and stiffened-box
-    requests (rate 10/s, size classes 0..4 = 5e3..2.5e4 DOF, per-request
+    requests (rate 20/s, size classes 0..4 = 5e3..2.5e4 DOF, per-request
     thickness field and load from the request seed), once with FP32 ILU
     factors (mixed) and once with FP64 factors, each to a 1e-8 relative
     residual. Size classes are built, their fill tuned and their slot groups
