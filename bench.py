@@ -272,7 +272,11 @@ SWEEP_TRAFFIC_RATIO = 1.055
 # batch autotuner (gpu_fem_b200/batch.py: ordering by ILU(8) levels x blocks
 # per row, then the converging k of smallest modelled factor + solve time) on
 # a B200. Both arms run every problem with these, so their configs match;
-# `--tune` re-runs the autotuner and prints the table it finds.
+# `--tune` re-runs the autotuner and prints the table it finds. This table
+# measured 268 solves/s; re-tuning with the current cost models picks higher
+# fills for the large plates (17 instead of 23 GMRES steps) and measured
+# 249 solves/s, because the batched factorization's time is not yet modelled
+# well enough (the problems share the SMs).
 FILLS = [12, 16, 12, 7, 6, 6, 10, 8, 8, 5, 8, 6, 10, 6, 12, 12, 8, 8, 8, 12, 12, 6, 10, 10, 6,
          16, 12, 6, 7, 8, 10, 12, 5, 12, 5, 10, 7, 6, 5, 12, 16, 16, 5, 12, 6, 10, 10, 12, 10,
          12, 8, 7, 16, 8, 6, 5, 8, 10, 12, 16, 4, 4, 10, 12]

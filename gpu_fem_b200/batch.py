@@ -90,7 +90,14 @@ def solve_opts(rtol=1e-8, mixed=False, restart=100, max_iters=20000, inner_rtol=
 ORDERINGS = ("natural", "rcm")
 
 
-def factor_cost_us(nrow, inf):
+def factor_work(nrow, inf):
+    """Block updates of one factorization: ~nrow x lower x (lower + 1), with
+    lower the blocks left of the diagonal per row."""
+    lower = max(inf["nnzb"] - nrow, 0) / (2.0 * nrow)
+    return nrow * lower * (lower + 1.0)
+
+
+def factor_cost_us(nrow, inf, warps=None):
     """One numeric factorization of a problem (microseconds), fitted to B200
     runs of single plates (16^2 to 256^2 elements, fills 1 to 16) on the
     dataflow factorization with dependency-ordered steps: ~7-9 us a lower
@@ -101,8 +108,9 @@ def factor_cost_us(nrow, inf):
     row) spread over the warps."""
     lvl, nnzb = inf["levels_L"], inf["nnzb"]
     lower = max(nnzb - nrow, 0) / (2.0 * nrow)
-    warps = 8 * max(1, min(128, nrow // 32))
-    work = nrow * lower * (lower + 1.0)
+    if warps is None:  # alone: up to 128 CTAs of 8 warps
+        warps = 8 * max(1, min(128, nrow // 32))
+    work = factor_work(nrow, inf)
     if inf.get("ordering", "natural") == "rcm":
         t = 7.19 * lvl - 0.0132 * lvl * lower + 0.0031 * lvl * lower * lower + 0.028 * work / warps - 2.9
     else:
@@ -153,6 +161,35 @@ def batch_cost_us(choice):
         run_max = max(run_max, sw)
     total += prev * (run_max + STEP_OVERHEAD_US)
     return fac + total
+
+
+def shared_factor_costs(cands, fills, sms=148):
+    """Candidates with the factor cost of a batched factorization: when the
+    problems' picks are `fills`, a candidate of problem p gets the SMs'
+    share (one 8-warp CTA each) that its block updates take of the batch's,
+    at most 128 CTAs. fills=None keeps the alone costs. Candidates without
+    their (nrow, info) keep their cost."""
+    if fills is None:
+        return [[c[:4] for c in cs] for cs in cands]
+    chosen = []
+    for cs, k in zip(cands, fills):
+        c = next(c for c in cs if c[0] == k)
+        chosen.append(factor_work(*c[4]) if len(c) > 4 else 0.0)
+    total = sum(chosen)
+    out = []
+    for p, cs in enumerate(cands):
+        row = []
+        for c in cs:
+            if len(c) <= 4 or total <= 0.0:
+                row.append(c[:4])
+                continue
+            nrow, inf = c[4]
+            w = factor_work(nrow, inf)
+            share = w / max(total - chosen[p] + w, 1e-30)
+            ctas = max(1, min(128, nrow // 32, int(sms * share)))
+            row.append((c[0], c[1], factor_cost_us(nrow, inf, warps=8 * ctas), c[3]))
+        out.append(row)
+    return out
 
 
 def choose_batch_fills(cands, rounds=8):
@@ -269,7 +306,7 @@ class BatchSolver:
             log.append((i, k, s["iterations"], s["rel_residual"], nlev, ok))
             if ok:
                 cands[i].append((k, s["iterations"], factor_cost_us(nrow, inf),
-                                 sweep_cost_us(inf)))
+                                 sweep_cost_us(inf), (nrow, inf)))
                 cost = step_cost_us(nrow, inf, s["iterations"])
                 if best[i] is None or cost < best[i][0]:
                     best[i] = (cost, k, k)
@@ -304,7 +341,15 @@ class BatchSolver:
                     and k > max(c[0] for c in cands[i])]
             if todo:
                 self._trial(k, todo, cap, best, cands, log)
-        fills, _ = choose_batch_fills(cands)
+        fills, _ = choose_batch_fills(shared_factor_costs(cands, fills=None))
+        # the batch's factorizations share the SMs in proportion to their
+        # block updates: re-cost every candidate with its share of the SMs
+        # given the other problems' picks, and choose again
+        for _ in range(3):
+            new, _ = choose_batch_fills(shared_factor_costs(cands, fills))
+            if new == fills:
+                break
+            fills = new
         return fills, log
 
     def step(self, mixed: bool, host_io=None, spmv32=False, phases=None):

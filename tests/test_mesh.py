@@ -83,3 +83,18 @@ def test_batch_objective_lowers_fill_of_early_converging_problems():
     from gpu_fem_b200.batch import STEP_OVERHEAD_US
     own = min(fast, key=lambda t: t[2] + t[1] * (t[3] + STEP_OVERHEAD_US))
     assert own[0] == 8
+
+
+def test_shared_factor_costs_charge_the_sm_share():
+    """In a batch the factorization's CTAs are shared out by block updates:
+    a heavy candidate of one problem among heavy others gets fewer SMs and
+    costs more than alone; without the others it costs what it costs alone."""
+    from gpu_fem_b200.batch import factor_cost_us, shared_factor_costs
+    n = 20000
+    inf = {"levels_L": 2000, "levels_U": 2000, "nnzb": 30 * n, "ordering": "natural"}
+    cand = (12, 20, factor_cost_us(n, inf), 500.0, (n, inf))
+    alone = shared_factor_costs([[cand]], [12])[0][0][2]
+    assert abs(alone - factor_cost_us(n, inf, warps=8 * 128)) < 1e-9
+    crowd = shared_factor_costs([[cand]] * 8, [12] * 8)[0][0][2]
+    assert crowd > alone
+    assert shared_factor_costs([[cand]], None)[0][0] == cand[:4]
