@@ -273,8 +273,15 @@ class BatchSolver:
             self.fills, self.tune_log = [0] * n, None
         if not build:  # fill levels only (the server tunes its size classes this way)
             return
-        self.P64 = [ILUk_Preconditioner(a, k, "fp64") for a, k in zip(self.asms, self.fills)]
-        self.P32 = [ILUk_Preconditioner(a, k, "fp32") for a, k in zip(self.asms, self.fills)]
+        # the preconditioners' host setup (orderings of the steps, chunk
+        # streams) runs in the library with the GIL released: build them on
+        # host threads
+        from concurrent.futures import ThreadPoolExecutor
+        jobs = [(a, k, pr) for pr in ("fp64", "fp32") for a, k in zip(self.asms, self.fills)]
+        with ThreadPoolExecutor(max_workers=min(8, len(jobs))) as ex:
+            built = list(ex.map(lambda j: ILUk_Preconditioner(*j), jobs))
+        n = len(self.asms)
+        self.P64, self.P32 = built[:n], built[n:]
         self.b64 = Batch(self.asms, self.mats, self.P64)
         self.b32 = Batch(self.asms, self.mats, self.P32)
         torch.cuda.synchronize()
