@@ -249,15 +249,21 @@ class BatchSolver:
         # own factor + solve time
         self.objective = objective
         self.meshes = meshes
+        # assemblers (host symbolic work in the library, GIL released) are
+        # built on host threads
+        from concurrent.futures import ThreadPoolExecutor
+        workers = max(1, min(8, len(meshes)))
         if ordering == "auto":
-            picked = [choose_ordering(m) for m in meshes]
+            with ThreadPoolExecutor(max_workers=workers) as ex:
+                picked = list(ex.map(choose_ordering, meshes))
             self.orderings = [o for o, _ in picked]
             self.asms = [a for _, a in picked]
         else:  # one ordering for all, or one per problem
             self.orderings = ([ordering] * len(meshes) if isinstance(ordering, str)
                               else list(ordering))
-            self.asms = [ElementAssembler.from_mesh(m, ordering=o)
-                         for m, o in zip(meshes, self.orderings)]
+            with ThreadPoolExecutor(max_workers=workers) as ex:
+                self.asms = list(ex.map(lambda mo: ElementAssembler.from_mesh(mo[0], ordering=mo[1]),
+                                        zip(meshes, self.orderings)))
         self.mats = [BsrMat(a) for a in self.asms]
         self.bs = [torch.tensor(m.loads, device="cuda") for m in meshes]
         self.xs = [torch.zeros_like(b) for b in self.bs]

@@ -772,12 +772,15 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
     double* rs = xs + 6 * (size_t)T.capb;
     // asynchronous copies for chunk c+1 (waited for one chunk later): far x
     // entries (rows solved by chunks <= c-1, complete at the barrier above)
-    // and right-hand sides
-    {
+    // and right-hand sides, into the gather area chunk c-1 used. When the
+    // chunk has fewer rows than the CTA has warps, the warps without a row
+    // issue them while the others solve theirs; otherwise every thread
+    // issues them first.
+    auto issue_next = [&](int t0, int stride) {
       double* xn = xbuf + xstride * ((c + 1) & 1);
       with_pw([&](auto pwc) {
         constexpr int pw = decltype(pwc)::value;
-        for (int t = tid; t < pw * (nf1 + nr1); t += kSweepThreads) {
+        for (int t = t0; t < pw * (nf1 + nr1); t += stride) {
           if (t < pw * nf1) {
             const int2 f = far1[t / pw];
             copy_piece(pwc, xn + 6 * f.x, ob + 6 * (size_t)f.y, t % pw);
@@ -788,8 +791,9 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
           }
         }
       });
-      cp_async_commit();
-    }
+    };
+    const bool idle_issue = nr < nw;
+    if (!idle_issue) issue_next(tid, kSweepThreads);
     // near entries: results of chunk c-1 from the ring
     {
       const double2* rp =
@@ -811,6 +815,8 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
       }
       issued++;
     }
+    if (idle_issue && warp >= nr) issue_next(tid - 32 * nr, 32 * (nw - nr));
+    cp_async_commit();
     double* wp = ring + 6 * (size_t)ringrows * (c & 1);
     const unsigned pwp = pring + 8u * 6u * (unsigned)ringrows * (unsigned)(c & 1);
     for (int k = warp; k < nr; k += nw) {
