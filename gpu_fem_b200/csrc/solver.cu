@@ -823,6 +823,13 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
       const int4 row = ri[k];
       const int i = row.x, rbeg = row.y, rcnt = row.z, gk = row.w;
       const int first = UPPER ? 1 : 0;  // U rows start with U_ii^{-1}
+      // row `lane` of U_ii^{-1} (lanes 0..5), loaded while the products run
+      double di[6];
+      if (UPPER) {
+        const VT* Di = sv + (size_t)rbeg * 36 + 6 * (lane < 6 ? lane : 0);
+#pragma unroll
+        for (int cc = 0; cc < 6; cc++) di[cc] = (double)Di[cc];
+      }
       double acc = 0.0;
       if (g < 4) {
         double acc1 = 0.0;
@@ -839,13 +846,11 @@ __global__ void __launch_bounds__(kSweepThreads) bsweep_tma(const ProbDev* __res
       const double t = (lane < 6 ? rs[6 * k + lane] : 0.0) - acc;
       double v = t;
       if (UPPER) {
-        const VT* Di = sv + (size_t)rbeg * 36;
-        v = 0.0;
+        double tc[6];
 #pragma unroll
-        for (int cc = 0; cc < 6; cc++) {
-          const double tc = __shfl_sync(0xffffffffu, t, cc);
-          if (lane < 6) v = fma((double)Di[6 * lane + cc], tc, v);
-        }
+        for (int cc = 0; cc < 6; cc++) tc[cc] = __shfl_sync(0xffffffffu, t, cc);
+        v = fma(di[4], tc[4], fma(di[2], tc[2], di[0] * tc[0])) +
+            fma(di[5], tc[5], fma(di[3], tc[3], di[1] * tc[1]));
       }
       if (lane < 6) {
         ob[6 * (size_t)i + lane] = v;
