@@ -231,7 +231,9 @@ gf_status gf_precond_create(gf_assembler* a, int32_t fill_level, int32_t precisi
  *                     it multiplies (shared-memory result ring), no block
  *                     barriers between levels;
  *  GF_SWEEP_LEVEL     level-synchronous chunks, split over a 2-CTA cluster
- *                     when levels are large;
+ *                     when a chunk-cost model says it pays (levels with
+ *                     more rows than one CTA's warps or more blocks than its
+ *                     stage);
  *  GF_SWEEP_AUTO      the level-synchronous kernel (the faster of the two
  *                     on the batched plate workload on B200).
  * The dataflow kernel needs its result ring and stages to fit one CTA's
@@ -251,7 +253,10 @@ gf_status gf_precond_destroy(gf_precond* p);
 gf_status gf_precond_sweeps(const gf_precond* p, int32_t* kind_L, int32_t* kind_U,
                             int32_t* ring_L, int32_t* ring_U);
 /* copyValues + numeric factorization (precond.h:35-44; cusparseDbsrilu02 at
- * examples/iterative/gmres.cu:426-457). Level-scheduled on the device. */
+ * examples/iterative/gmres.cu:426-457). A dataflow kernel on the device: one
+ * warp per row, rows taken in level order, each step waiting only for the
+ * row it reads (bounded waits; GF_TIMEOUT if one runs out). The factor is
+ * bitwise reproducible run to run. */
 gf_status gf_precond_factor(gf_precond* p, gf_bsr* A, void* stream);
 /* z = U^{-1} L^{-1} r (two cusparseDbsrsv2_solve calls,
  * examples/iterative/gmres.cu:522-532), solver ordering. */
