@@ -22,10 +22,13 @@
 //    goes into the Jacobian column, so K is the exact Hessian of the energy and
 //    R(u) = K u (pinned by the complex-step tests).
 //
-// parity is pinned by: complex-step residual/energy and Jacobian/residual
-// identities on the reference's one-element fixture, the 2-element fill-in
-// known answer, linearity/symmetry/rigid-body properties, and the Navier
-// plate solution (see tests/).
+// Parity unpinned by reference outputs: the reference cannot be built here
+// (A2D and sparse-utils are absent) and its tests store no expected values.
+// What the restatement is checked against instead: complex-step
+// residual/energy and Jacobian/residual identities on the reference's
+// one-element fixture, the 2-element fill-in known answer,
+// linearity/symmetry/rigid-body properties, and the Navier plate solution
+// (see tests/).
 #pragma once
 #include <cmath>
 #include <complex>
