@@ -381,10 +381,15 @@ gf_status gf_direct_solve(gf_assembler* a, gf_bsr* A, const double* d_b, double*
 gf_status gf_batch_create(int32_t n, gf_assembler* const* asms, gf_bsr* const* mats,
                           gf_precond* const* pcs, gf_batch** out);
 gf_status gf_batch_destroy(gf_batch* b);
-/* add_jacobian with fused BCs for every problem. */
+/* add_jacobian with fused BCs for every problem: one launch per colour over
+ * all problems (or one launch with gf_batch_set_scatter(GF_ASSEMBLE_ATOMIC)).
+ * The per-problem launch parameters are cached in the batch and uploaded
+ * again (with a synchronisation of `stream`) only when they change. Calls on
+ * one batch must not overlap. */
 gf_status gf_batch_assemble(gf_batch* b, void* stream);
 /* As gf_batch_assemble with a per-problem thickness field (d_thick[k] may be
- * NULL to use the assembler's own). */
+ * NULL to use the assembler's own). Passing the same pointers every call
+ * keeps the cached parameters; new pointers re-upload them. */
 gf_status gf_batch_assemble_ex(gf_batch* b, const double* const* d_thick, void* stream);
 /* Numeric ILU(k) of every problem in one level-ordered launch. */
 /* Scatter of the batch's assembly (gf_batch_assemble / _ex): 0 (default)
