@@ -112,6 +112,7 @@ SIGNATURES = {
     "gf_precond_status": (_I, [_P, _P]),
     "gf_precond_layout": (_I, [_P, _PI, _PI, _PI, _PI, _PI]),
     "gf_batch_set_scatter": (_I, [_P, C.c_int32]),
+    "gf_assembler_setup_info": (_I, [_P, _PI, _PI]),
     "gf_precond_setup_info": (_I, [_P, _PI, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "gf_test_set_waits": (_I, [C.c_ulonglong, _I]),
     "gf_precond_get": (_I, [_P, _PI, _PI, _PD]),

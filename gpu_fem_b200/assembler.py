@@ -206,6 +206,13 @@ class ElementAssembler:
         rp = None if res is None else res.getPtr()
         check(L.lib().gf_add_jacobian(self.h, rp, mat.h, flags, _stream()), "add_jacobian")
 
+    def setup_info(self):
+        """gf_assembler_setup_info: whether the node pattern and the
+        elemIndMap were computed on the GPU."""
+        p, m = C.c_int32(), C.c_int32()
+        check(L.lib().gf_assembler_setup_info(self.h, C.byref(p), C.byref(m)), "setup_info")
+        return {"pattern_on_gpu": bool(p.value), "elem_map_on_gpu": bool(m.value)}
+
     def tune_scatter(self, mat, reps=5):
         """Times the Jacobian with the coloured and the atomic scatter on
         `mat` and keeps the faster for add_jacobian(atomic=None); returns the

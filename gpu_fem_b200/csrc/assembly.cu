@@ -508,12 +508,18 @@ gf_status gf_assembler_create(const gf_mesh_desc* d, gf_assembler** out) {
   a->nbcs = d->num_bcs;
   a->conn.assign(d->conn, d->conn + 4 * (size_t)ne);
   a->bcs.assign(d->bcs, d->bcs + d->num_bcs);
-  a->pat0 = pattern_from_conn(ne, nn, d->conn);
+  if (pattern_from_conn_gpu(ne, nn, d->conn, a->pat0))
+    a->sym_flags |= 1;
+  else
+    a->pat0 = pattern_from_conn(ne, nn, d->conn);
   order_nodes(a->pat0, d, a->perm);
   a->iperm.resize(nn);
   for (int i = 0; i < nn; i++) a->iperm[a->perm[i]] = i;
   a->pat = permute_pattern(a->pat0, a->perm);
-  elem_ind_map(ne, d->conn, a->pat, a->perm, a->emap);
+  if (elem_ind_map_gpu(ne, d->conn, a->pat, a->perm, a->emap))
+    a->sym_flags |= 2;
+  else
+    elem_ind_map(ne, d->conn, a->pat, a->perm, a->emap);
   if (build_schedule(ne, nn, d->conn, a->emap, a->pat.nnz(), kChunkSize, a->sched) != 0) {
     delete a;
     return GF_INVALID_ARG;
@@ -656,6 +662,14 @@ gf_status gf_set_variables(gf_assembler* a, const double* d_vars, void* stream) 
 gf_status gf_add_residual(gf_assembler* a, double* d_res, int32_t flags, void* stream) {
   if (!a || !d_res) return GF_INVALID_ARG;
   return launch_assembly<MODE_RES>(a, nullptr, d_res, flags, as_stream(stream));
+}
+
+gf_status gf_assembler_setup_info(const gf_assembler* a, int32_t* pattern_on_gpu,
+                                  int32_t* elem_map_on_gpu) {
+  if (!a) return GF_INVALID_ARG;
+  if (pattern_on_gpu) *pattern_on_gpu = (a->sym_flags & 1) ? 1 : 0;
+  if (elem_map_on_gpu) *elem_map_on_gpu = (a->sym_flags & 2) ? 1 : 0;
+  return GF_OK;
 }
 
 gf_status gf_add_jacobian(gf_assembler* a, double* d_res, gf_bsr* mat, int32_t flags,

@@ -93,6 +93,12 @@ Pattern iluk_pattern(const Pattern& a, int lev);
 // column window exceeds the kernel's or the device fails, and the caller
 // then uses iluk_pattern.
 bool iluk_pattern_gpu(const Pattern& a, int lev, Pattern& out);
+// The node pattern and elemIndMap computed on the GPU (symbolic_gpu.cu):
+// false when a node has more than 64 elements or the device fails, and the
+// caller then uses pattern_from_conn / elem_ind_map.
+bool pattern_from_conn_gpu(int nelem, int nnodes, const int32_t* conn, Pattern& out);
+bool elem_ind_map_gpu(int nelem, const int32_t* conn, const Pattern& p,
+                      const std::vector<int32_t>& perm, std::vector<int32_t>& map);
 // Level sets of the lower / upper triangular DAG.
 int levels(const Pattern& p, bool lower, std::vector<int32_t>& level);
 
@@ -182,6 +188,7 @@ int build_schedule(int nelem, int nnodes, const int32_t* conn, const std::vector
 // ------------------------------------------------------------------ handles
 struct gf_assembler {
   int nnodes = 0, nelem = 0, nbcs = 0;
+  int sym_flags = 0;                // bit 0: node pattern, bit 1: elemIndMap computed on the GPU
   gf::Pattern pat0;                 // natural pattern
   gf::Pattern pat;                  // solver-order pattern
   std::vector<int32_t> perm, iperm;

@@ -147,7 +147,182 @@ __global__ void iluk_sym_compact(int n, const int64_t* __restrict__ off,
   for (int t = lane; t < c; t += 32) cols[rowp[i] + t] = ocols[off[i] + t];
 }
 
+// ---- node pattern and elemIndMap
+// (get_row_col_ptrs, include/linalg/bsr_utils.h:430-476; get_elem_ind_map,
+// include/linalg/bsr_utils.h:809-870)
+constexpr int kNodeCand = 256;  // candidate neighbours of a node (4 per incident element)
+
+__global__ void node_incidence(int nelem, const int32_t* __restrict__ conn, int32_t* cnt) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nelem) return;
+  for (int a = 0; a < 4; a++) atomicAdd(&cnt[conn[4 * e + a]], 1);
+}
+
+__global__ void node_elements(int nelem, const int32_t* __restrict__ conn,
+                              const int32_t* __restrict__ start, int32_t* cursor, int32_t* elems) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nelem) return;
+  for (int a = 0; a < 4; a++) {
+    const int v = conn[4 * e + a];
+    elems[start[v] + atomicAdd(&cursor[v], 1)] = e;
+  }
+}
+
+// One warp per node: the nodes of its elements, deduplicated and sorted by
+// rank (a candidate's position is the number of distinct smaller ones).
+// rowp == nullptr: count only.
+__global__ void __launch_bounds__(256)
+    node_rows(int nnodes, const int32_t* __restrict__ conn, const int32_t* __restrict__ start,
+              const int32_t* __restrict__ elems, int32_t* cnt, const int32_t* __restrict__ rowp,
+              int32_t* cols) {
+  __shared__ int32_t cand[8][kNodeCand];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i = blockIdx.x * 8 + warp;
+  if (i >= nnodes) return;
+  int32_t* cd = cand[warp];
+  const int e0 = start[i], m = 4 * (start[i + 1] - e0);
+  for (int t = lane; t < m; t += 32) cd[t] = conn[4 * elems[e0 + t / 4] + t % 4];
+  __syncwarp();
+  int nuniq = 0;
+  for (int t0 = 0; t0 < m; t0 += 32) {
+    const int t = t0 + lane;
+    bool first = t < m;
+    int pos = 0;
+    if (first) {
+      const int v = cd[t];
+      for (int s = 0; s < t && first; s++) first = cd[s] != v;
+      if (first && rowp)
+        for (int s = 0; s < m; s++) {
+          const int w = cd[s];
+          if (w < v) {
+            bool f2 = true;
+            for (int u = 0; u < s && f2; u++) f2 = cd[u] != w;
+            pos += f2 ? 1 : 0;
+          }
+        }
+      if (first && rowp) cols[rowp[i] + pos] = v;
+    }
+    nuniq += __popc(__ballot_sync(0xffffffffu, first));
+  }
+  if (lane == 0 && !rowp) cnt[i] = nuniq;
+}
+
+// 16 entries per element: slot of block (perm[node a], perm[node b]).
+__global__ void elem_map_kernel(int nelem, const int32_t* __restrict__ conn,
+                                const int32_t* __restrict__ perm, const int32_t* __restrict__ rowp,
+                                const int32_t* __restrict__ cols, int32_t* map) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (size_t)16 * nelem) return;
+  const int e = (int)(t / 16), a = (int)(t % 16) / 4, b = (int)(t % 4);
+  const int r = perm[conn[4 * e + a]], c = perm[conn[4 * e + b]];
+  int lo = rowp[r], hi = rowp[r + 1];
+  const int end = hi;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (cols[mid] < c)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  map[t] = (lo < end && cols[lo] == c) ? lo : -1;
+}
+
 }  // namespace
+
+bool pattern_from_conn_gpu(int nelem, int nnodes, const int32_t* conn, Pattern& out) {
+  if (nelem <= 0 || nnodes <= 0) return false;
+  DevBuf<int32_t> d_conn, d_cnt, d_start, d_cursor, d_elems, d_rows, d_rowp, d_cols;
+  cudaError_t e = cudaSuccess;
+  auto up = [&](cudaError_t x) {
+    if (e == cudaSuccess) e = x;
+  };
+  up(d_conn.upload(conn, (size_t)4 * nelem));
+  up(d_cnt.alloc(nnodes));
+  if (e == cudaSuccess) up(cudaMemset(d_cnt.p, 0, sizeof(int32_t) * nnodes));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  const unsigned eb = (unsigned)((nelem + 255) / 256), nb = (unsigned)((nnodes + 7) / 8);
+  count_launch();
+  node_incidence<<<eb, 256>>>(nelem, d_conn.p, d_cnt.p);
+  std::vector<int32_t> cnt(nnodes), start(nnodes + 1, 0);
+  up(cudaMemcpy(cnt.data(), d_cnt.p, sizeof(int32_t) * nnodes, cudaMemcpyDeviceToHost));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  for (int i = 0; i < nnodes; i++) {
+    if (4 * cnt[i] > kNodeCand) return false;  // the host handles such meshes
+    start[i + 1] = start[i] + cnt[i];
+  }
+  up(d_start.upload(start));
+  up(d_cursor.alloc(nnodes));
+  up(d_elems.alloc((size_t)start[nnodes]));
+  if (e == cudaSuccess) up(cudaMemset(d_cursor.p, 0, sizeof(int32_t) * nnodes));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  count_launch();
+  node_elements<<<eb, 256>>>(nelem, d_conn.p, d_start.p, d_cursor.p, d_elems.p);
+  count_launch();
+  node_rows<<<nb, 256>>>(nnodes, d_conn.p, d_start.p, d_elems.p, d_cnt.p, nullptr, nullptr);
+  up(cudaMemcpy(cnt.data(), d_cnt.p, sizeof(int32_t) * nnodes, cudaMemcpyDeviceToHost));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  out.n = nnodes;
+  out.rowp.assign(nnodes + 1, 0);
+  for (int i = 0; i < nnodes; i++) out.rowp[i + 1] = out.rowp[i] + cnt[i];
+  up(d_rowp.upload(out.rowp));
+  up(d_cols.alloc((size_t)out.rowp[nnodes]));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  count_launch();
+  node_rows<<<nb, 256>>>(nnodes, d_conn.p, d_start.p, d_elems.p, d_cnt.p, d_rowp.p, d_cols.p);
+  out.cols.resize(out.rowp[nnodes]);
+  up(cudaGetLastError());
+  up(cudaMemcpy(out.cols.data(), d_cols.p, sizeof(int32_t) * out.cols.size(),
+                cudaMemcpyDeviceToHost));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return true;
+}
+
+bool elem_ind_map_gpu(int nelem, const int32_t* conn, const Pattern& p,
+                      const std::vector<int32_t>& perm, std::vector<int32_t>& map) {
+  DevBuf<int32_t> d_conn, d_perm, d_rowp, d_cols, d_map;
+  cudaError_t e = cudaSuccess;
+  auto up = [&](cudaError_t x) {
+    if (e == cudaSuccess) e = x;
+  };
+  up(d_conn.upload(conn, (size_t)4 * nelem));
+  up(d_perm.upload(perm));
+  up(d_rowp.upload(p.rowp));
+  up(d_cols.upload(p.cols));
+  up(d_map.alloc((size_t)16 * nelem));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  count_launch();
+  elem_map_kernel<<<(unsigned)(((size_t)16 * nelem + 255) / 256), 256>>>(nelem, d_conn.p, d_perm.p,
+                                                                       d_rowp.p, d_cols.p, d_map.p);
+  map.resize((size_t)16 * nelem);
+  up(cudaGetLastError());
+  up(cudaMemcpy(map.data(), d_map.p, sizeof(int32_t) * map.size(), cudaMemcpyDeviceToHost));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return true;
+}
 
 bool iluk_pattern_gpu(const Pattern& a, int fill, Pattern& out) {
   const int n = a.n;

@@ -127,6 +127,13 @@ gf_status gf_assembler_create(const gf_mesh_desc* desc, gf_assembler** out);
 /* The node ordering gf_assembler_create would use for this mesh
  * (perm[natural node] = solver row, num_nodes entries). Host only: needs no
  * GPU. */
+/* Which parts of the assembler's symbolic setup ran on the GPU: the node
+ * pattern (get_row_col_ptrs, include/linalg/bsr_utils.h:430-476) and the
+ * elemIndMap (get_elem_ind_map, :809-870); 0 where the host computed them (a
+ * node with more than 64 elements, or a device failure). Any pointer may be
+ * NULL. The node ordering and the scatter colouring are host algorithms. */
+gf_status gf_assembler_setup_info(const gf_assembler* a, int32_t* pattern_on_gpu,
+                                  int32_t* elem_map_on_gpu);
 gf_status gf_order_nodes(const gf_mesh_desc* desc, int32_t* perm);
 gf_status gf_assembler_destroy(gf_assembler* a);
 /* get_num_nodes / get_num_elements / get_num_vars (include/assembler.h:117-118, :309-310) */

@@ -1,8 +1,9 @@
-"""ILU(k) symbolic factorization on the GPU (gf_precond_create ->
+"""Symbolic setup on the GPU. ILU(k) symbolic factorization (gf_precond_create ->
 iluk_pattern_gpu): the pattern is bit-exact against the oracle's restatement
 of computeILUk (include/linalg/bsr_utils.h:678-807) for natural, RCM and
 q-ordered plates, a stiffened box and the complete factor (GF_FILL_FULL),
-and gf_precond_setup_info reports that the GPU computed it."""
+and gf_precond_setup_info reports that the GPU computed it. Node pattern and
+elemIndMap of gf_assembler_create, bit-exact, with gf_assembler_setup_info."""
 import numpy as np
 import pytest
 
@@ -52,3 +53,24 @@ def test_gpu_complete_factor_pattern():
     assert P.setup_info()["symbolic_on_gpu"]
     r, c, _ = P.get()
     assert r[-1] == po.full_fill_count(bd["rowPtr"], bd["colPtr"])
+
+
+@pytest.mark.parametrize("kind,ordering", [("plate", "natural"), ("plate", "rcm"),
+                                           ("jittered", "rcm"), ("box", "rcm")])
+def test_gpu_node_pattern_and_elem_map_match_oracle(kind, ordering):
+    """Node pattern (get_row_col_ptrs) and elemIndMap (get_elem_ind_map) built
+    on the GPU by gf_assembler_create: bit-exact against the oracle in the
+    solver ordering."""
+    from gpu_fem_b200.assembler import ElementAssembler
+    from oracle import pyoracle as po
+    mesh = {"plate": lambda: _plate(40, 24), "jittered": lambda: M.plate_config2(30, 15),
+            "box": lambda: M.box(18, 6, 4)}[kind]()
+    A = ElementAssembler.from_mesh(mesh, ordering=ordering)
+    info = A.setup_info()
+    assert info["pattern_on_gpu"] and info["elem_map_on_gpu"], info
+    bd = A.getBsrData()
+    r0, c0 = po.bsr_pattern(mesh.conn, mesh.num_nodes)
+    rp, cp = po.permute_pattern(r0, c0, bd["perm"])[:2]
+    np.testing.assert_array_equal(bd["rowPtr"], rp)
+    np.testing.assert_array_equal(bd["colPtr"], cp)
+    np.testing.assert_array_equal(bd["elemIndMap"], po.elem_ind_map(mesh.conn, rp, cp, bd["perm"]))
