@@ -2033,18 +2033,21 @@ static int fac_ctas_cap(const gf_precond* p, int budget) {
 static int fac_ctas_alone(const gf_precond* p) { return fac_ctas_cap(p, sm_count()); }
 
 // Spreads one CTA per SM over the batch's problems in proportion to their
-// block updates (largest remainders first), within each problem's cap;
+// block updates to the power 0.7 (largest remainders first), within each
+// problem's cap: the small problems' dependency chains need a few CTAs more
+// than their share of the updates (64-plate batch on B200: 41.4 ms with
+// shares by updates, 38.1 ms with 0.7, 56.6 ms with 1.5);
 // fills cta_prob with the problem of every CTA.
 static void fac_plan(const std::vector<gf_precond*>& pcs, std::vector<int>& ctas,
                      std::vector<int32_t>& cta_prob) {
   const int np = (int)pcs.size(), total = std::max(sm_count(), np);
   double W = 0.0;
-  for (auto* p : pcs) W += (double)std::max<long long>(p->fwork, 1);
+  for (auto* p : pcs) W += std::pow((double)std::max<long long>(p->fwork, 1), 0.7);
   ctas.assign(np, 1);
   std::vector<std::pair<double, int>> rem;
   int used = 0;
   for (int k = 0; k < np; k++) {
-    const double want = total * (double)std::max<long long>(pcs[k]->fwork, 1) / W;
+    const double want = total * std::pow((double)std::max<long long>(pcs[k]->fwork, 1), 0.7) / W;
     const int cap = fac_ctas_cap(pcs[k], total);
     ctas[k] = std::max(1, std::min(cap, (int)want));
     used += ctas[k];
