@@ -167,14 +167,16 @@ def shared_factor_costs(cands, fills, sms=148):
     """Candidates with the factor cost of a batched factorization: when the
     problems' picks are `fills`, a candidate of problem p gets the SMs'
     share (one 8-warp CTA each) that its block updates take of the batch's,
-    at most 128 CTAs. fills=None keeps the alone costs. Candidates without
+    at most 128 CTAs (weights: block updates ** 0.7, as in the library's
+    plan). fills=None keeps the alone costs. Candidates without
     their (nrow, info) keep their cost."""
     if fills is None:
         return [[c[:4] for c in cs] for cs in cands]
+    # the library's CTA plan weights problems by block updates ** 0.7
     chosen = []
     for cs, k in zip(cands, fills):
         c = next(c for c in cs if c[0] == k)
-        chosen.append(factor_work(*c[4]) if len(c) > 4 else 0.0)
+        chosen.append(factor_work(*c[4]) ** 0.7 if len(c) > 4 else 0.0)
     total = sum(chosen)
     out = []
     for p, cs in enumerate(cands):
@@ -184,7 +186,7 @@ def shared_factor_costs(cands, fills, sms=148):
                 row.append(c[:4])
                 continue
             nrow, inf = c[4]
-            w = factor_work(nrow, inf)
+            w = factor_work(nrow, inf) ** 0.7
             share = w / max(total - chosen[p] + w, 1e-30)
             ctas = max(1, min(128, nrow // 32, int(sms * share)))
             row.append((c[0], c[1], factor_cost_us(nrow, inf, warps=8 * ctas), c[3]))
