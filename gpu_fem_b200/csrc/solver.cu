@@ -2035,8 +2035,8 @@ static int fac_ctas_alone(const gf_precond* p) { return fac_ctas_cap(p, sm_count
 // Spreads one CTA per SM over the batch's problems in proportion to their
 // block updates to the power 0.7 (largest remainders first), within each
 // problem's cap: the small problems' dependency chains need a few CTAs more
-// than their share of the updates (64-plate batch on B200: 41.4 ms with
-// shares by updates, 38.1 ms with 0.7, 56.6 ms with 1.5);
+// than their share of the updates (64-plate batch on B200, factorization
+// ms by exponent: 0.5 43.3, 0.6 40.1, 0.7 38.0, 0.85 39.2, 1 41.4, 1.5 56.6);
 // fills cta_prob with the problem of every CTA.
 static void fac_plan(const std::vector<gf_precond*>& pcs, std::vector<int>& ctas,
                      std::vector<int32_t>& cta_prob) {
